@@ -1,0 +1,185 @@
+/* vdi.h — C ABI of the B200 implementation of vdropimpact's per-timestep
+ * fluid solve.
+ *
+ * Every entry point returns an int status (VDI_OK = 0). Nothing here exits
+ * the process: where the reference calls fatal_error() (common.cc:44-47) the
+ * library returns an error status instead.
+ *
+ * Pointers named d_* are device pointers (CUDA global memory on the current
+ * device); pointers named h_* are host pointers. A stream argument of NULL
+ * means the legacy default stream. No torch or CUDA C++ types appear here.
+ *
+ * Array layouts follow the reference:
+ *   - a liquid-grid field with ghost layers is (n+4) rows of (m+4) doubles,
+ *     row-major, cell (i,j) at [(j+2)*(m+4) + i+2] (fluid_2d.cc:15-18);
+ *   - a multigrid solution/source over an m x n grid is m*n values with
+ *     ij = i + m*j (mgs_common.cc:8-10);
+ *   - tridiagonal systems are four arrays a (sub, a[0] unused), b (diagonal),
+ *     c (super, c[n-1] unused) and d (right-hand side, overwritten with the
+ *     solution), as tri_solve (tri_solve.hh:6-22).
+ */
+#ifndef VDI_H
+#define VDI_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VDI_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status */
+enum vdi_status {
+    VDI_OK = 0,
+    VDI_ERR_INVALID_ARGUMENT = 1,   /* bad pointer, size or option */
+    VDI_ERR_UNSUPPORTED_SIZE = 2,   /* grid the multigrid hierarchy cannot coarsen */
+    VDI_ERR_CUDA = 3,               /* a CUDA runtime call failed */
+    VDI_ERR_OUT_OF_MEMORY = 4,
+    VDI_ERR_MG_NOT_CONVERGED = 5,   /* V-cycle cap reached (mgs_mac.hh:68-70) */
+    VDI_ERR_NEWTON_NOT_CONVERGED = 6, /* > 256 Newton steps (gas_layer_solve.cc:204) */
+    VDI_ERR_TRI_SINGULAR = 7,       /* zero pivot (dgtsv info != 0, tri_solve.cc:29-32) */
+    VDI_ERR_NONFINITE = 8,          /* NaN/Inf in a residual */
+    VDI_ERR_CONFIG = 9,             /* configuration text not understood (fileinfo.cc) */
+    VDI_ERR_NOT_READY = 10          /* call order violated */
+};
+
+/* Returns a static string for a status code. */
+const char* vdi_status_string(int status);
+/* Returns VDI_ABI_VERSION. */
+int vdi_abi_version(void);
+/* Detail of the most recent error on the calling thread (static buffer). */
+const char* vdi_last_error(void);
+
+/* ------------------------------------------------------------ parameters
+ * The drop-impact parameters after fileinfo's unit conversion
+ * (fileinfo.cc:142-152), plus the numerical options of this library. */
+typedef struct vdi_params {
+    int m, n;                 /* liquid grid cells (fileinfo.hh:20-22) */
+    int x_sym;                /* symmetric about x=0 (fileinfo.hh:39) */
+    int implicit_visc;        /* Crank-Nicolson viscosity (fileinfo.hh:36) */
+    double ax, ay, bx, by;    /* domain */
+    double mu, rho;           /* liquid dynamic viscosity, density */
+    double tmult;             /* timestep padding factor */
+    double t_end;             /* simulation duration */
+    int nframes;              /* output frames (timestep fitting only) */
+    /* gas layer (gas_layer_solve.hh:21-41) */
+    double alpha, mug, Pamb, h0, R, V, sigma;
+    /* numerical options */
+    double mg_rtol;           /* relative residual ||b-Az||/||b|| ending a solve (1e-10) */
+    int mg_max_vcycles;       /* V-cycle cap per solve (default 200) */
+    int mg_precision;         /* VDI_MG_FP64 or VDI_MG_MIXED */
+    int mg_guess;             /* VDI_GUESS_EXTRAPOLATE or VDI_GUESS_LEARNED */
+} vdi_params;
+
+enum vdi_mg_precision {
+    VDI_MG_FP64 = 0,          /* FP64 V-cycles */
+    VDI_MG_MIXED = 1          /* FP32 V-cycles inside FP64 iterative refinement */
+};
+enum vdi_mg_guess {
+    VDI_GUESS_EXTRAPOLATE = 0, /* linear time extrapolation (mgs_common.cc:17-50) */
+    VDI_GUESS_LEARNED = 1      /* U-Net prediction added to the extrapolation */
+};
+
+/* Parses a vdropimpact .cfg text (fileinfo.cc:11-193; gas_layer_model only)
+ * into *out with the default numerical options. */
+int vdi_params_from_cfg(const char* cfg_text, vdi_params* out);
+
+/* --------------------------------------------------------- simulation */
+typedef struct vdi_sim vdi_sim;
+
+/* fluid_2d::fluid_2d (fluid_2d.cc:14-24): allocates the device state and
+ * sets up the four multigrid hierarchies on the current device. */
+int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out);
+int vdi_sim_destroy(vdi_sim* sim);
+/* fluid_2d::init_fields (fluid_2d_sio.cc:14-35) with the gas layer's
+ * init_fields (gas_layer_solve.cc:32-53). */
+int vdi_sim_init_fields(vdi_sim* sim);
+/* fluid_2d::timestep_select (fluid_2d.hh:82-86); also the frame timestep of
+ * fluid_2d::solve when interval = t_end/nframes. */
+int vdi_sim_timestep_select(const vdi_sim* sim, double interval, double* adt, int* nsteps);
+/* fluid_2d::step_forward (fluid_2d.cc:93-405), nsteps times with step dt.
+ * Asynchronous with respect to the host unless an error must be reported;
+ * the status of device-side checks is read at the end of the call. */
+int vdi_sim_step_forward(vdi_sim* sim, double dt, int nsteps);
+/* Captures one step_forward(dt) as a CUDA graph with device-side loops for
+ * the V-cycles and Newton steps; later vdi_sim_step_forward calls with the
+ * same dt replay it. enable=0 returns to eager launches. */
+int vdi_sim_use_graph(vdi_sim* sim, int enable);
+/* Blocks until queued work finishes; returns the first device-side error. */
+int vdi_sim_synchronize(vdi_sim* sim);
+
+/* Host copy of the state the reference writes to a restart file
+ * (fluid_2d_sio.cc:97-119, gas_layer_solve.cc:313-331): u, v, p over the
+ * ghosted grid ((n+4)*(m+4) each), the gas layer's liquid pressure gp[m+1],
+ * shear stress tau[m+4], height h[m], boundary flux fbd[m], gas pressure
+ * pg[m+1], height rate ht[m], plus time and Vframe. */
+typedef struct vdi_state {
+    double time, Vframe;
+    double *u, *v, *p;
+    double *gp, *tau, *h, *fbd, *pg, *ht;
+} vdi_state;
+int vdi_sim_get_state(vdi_sim* sim, vdi_state* h_state);
+int vdi_sim_set_state(vdi_sim* sim, const vdi_state* h_state);
+
+/* Per-solver statistics since the last reset (the reference's
+ * tgmg_predict::avg_iters and wall-clock counters, mgs_common.hh:47-55). */
+typedef struct vdi_stats {
+    long steps;
+    long solves[4];           /* MAC, FEM, VX, VY */
+    long vcycles[4];
+    long newton_steps;
+    long tri_pivot_fallbacks; /* tridiagonal solves that needed pivoting */
+    long height_fixed_point_iters;
+    double last_rel_res[4];
+} vdi_stats;
+int vdi_sim_stats(vdi_sim* sim, vdi_stats* out, int reset);
+
+/* Device pointers to the state arrays (read-only use by callers that keep
+ * data on the device). which: 0 u, 1 v, 2 p, 3 gas h, 4 gas pg, 5 gas gp. */
+int vdi_sim_device_field(vdi_sim* sim, int which, double** d_ptr, size_t* count);
+
+/* --------------------------------------------------------- multigrid
+ * A standalone linear system with the TGMG-style interface the reference's
+ * problem classes use (mgs_mac.hh, mgs_fem.hh, visco_impl.hh). */
+enum vdi_mg_kind {
+    VDI_MG_MAC = 0,           /* mgs_mac.hh:25-50: m x n cells, 5-point */
+    VDI_MG_FEM = 1,           /* mgs_fem.hh:42-57: m x n nodes, 9-point FE */
+    VDI_MG_VISC_U = 2,        /* visco_impl.hh:28-53, horizontal_vel = true */
+    VDI_MG_VISC_V = 3         /* visco_impl.hh:28-53, horizontal_vel = false */
+};
+typedef struct vdi_mg vdi_mg;
+/* MAC: c1 = dx, c2 = dy (mgs_mac.cc:23-27). FEM: c1 = dx, c2 = dy
+ * (mgs_fem.cc:26-30). VISC: c1 = vfx, c2 = vfy, x_sym as visco_impl. */
+int vdi_mg_create(int kind, int m, int n, double c1, double c2, int x_sym, void* stream, vdi_mg** out);
+int vdi_mg_destroy(vdi_mg* mg);
+/* tgmg::setup: builds the level hierarchy (also done by create). */
+int vdi_mg_setup(vdi_mg* mg);
+/* tgmg::solve_v_cycle: V-cycles on z (initial guess in, solution out) until
+ * ||b-Az||_2 <= rtol*||b||_2; precision is a vdi_mg_precision. */
+typedef struct vdi_mg_result {
+    int vcycles;
+    double rel_res;
+} vdi_mg_result;
+int vdi_mg_solve(vdi_mg* mg, const double* d_b, double* d_z, double rtol, int max_vcycles,
+                 int precision, vdi_mg_result* res);
+/* tgmg::v_cycle: one FP64 V-cycle on z. */
+int vdi_mg_v_cycle(vdi_mg* mg, const double* d_b, double* d_z);
+/* r = b - A z (the residual tgmg::output_res writes) and its 2-norm. */
+int vdi_mg_residual(vdi_mg* mg, const double* d_b, const double* d_z, double* d_r, double* norm);
+/* y = A z, the operator of the problem class (a_cc*z + mul_a). */
+int vdi_mg_apply(vdi_mg* mg, const double* d_z, double* d_y);
+
+/* ------------------------------------------------------- tridiagonal
+ * tri_solve::solve_lapack (tri_solve.cc:24-33): solves the n x n system in
+ * place (solution in d_d) on the GPU by cyclic reduction, falling back to
+ * Gaussian elimination with partial pivoting when a row is not diagonally
+ * dominant. a, b, c are overwritten. *pivoted is set to 1 when the fallback
+ * ran (may be NULL). */
+int vdi_tri_solve(int n, double* d_a, double* d_b, double* d_c, double* d_d, void* stream, int* pivoted);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

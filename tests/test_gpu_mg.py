@@ -1,0 +1,187 @@
+"""Multigrid parity on the GPU: the operators equal the reference's stencil
+accessors (mgs_mac.hh:33-45, mgs_fem.cc:32-53, visco_impl.hh:36-46), and
+solves reach ||b-Az||/||b|| <= rtol and agree with an exact sparse solve."""
+import numpy as np
+import pytest
+
+from oracle import vdi_oracle as vo
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def V():
+    import vdropimpact_b200 as V
+    return V
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def gaussians_rhs(m, n, seed, k=64):
+    """Zero-mean sum of k Gaussians (centres uniform, widths 0.01-0.1 of the
+    domain, amplitudes N(0,1)): the single-projection workload's RHS."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(m) + 0.5) / m
+    y = (np.arange(n) + 0.5) / n * (n / m)
+    X, Y = np.meshgrid(x, y)
+    b = np.zeros((n, m))
+    for _ in range(k):
+        cx, cy = rng.uniform(0, 1), rng.uniform(0, n / m)
+        w = rng.uniform(0.01, 0.1)
+        a = rng.standard_normal()
+        b += a * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * w * w))
+    return (b - b.mean()).ravel()
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("m,n", [(64, 32), (256, 128)])
+def test_mac_apply_equals_accessors(V, m, n):
+    torch = _torch()
+    dx, dy = 2. / (m - 1), 2. / (n - 1)
+    A = vo.mac_matrix(m, n, 1. / (dx * dx), 1. / (dy * dy))
+    s = V.MgsMac(m, n, dx, dy)
+    z = np.random.default_rng(1).standard_normal(m * n)
+    s.z.copy_(torch.from_numpy(z))
+    y = s.apply().cpu().numpy()
+    assert _rel(y, A @ z) < 1e-14
+
+
+@pytest.mark.parametrize("M,N", [(65, 33), (257, 129)])
+def test_fem_apply_equals_accessors(V, M, N):
+    torch = _torch()
+    dx, dy = 1e-3, 1.3e-3
+    A = vo.fem_matrix(M, N, dx, dy)
+    s = V.MgsFem(M, N, dx, dy)
+    z = np.random.default_rng(2).standard_normal(M * N)
+    s.z.copy_(torch.from_numpy(z))
+    y = s.apply().cpu().numpy()
+    assert _rel(y, A @ z) < 1e-14
+
+
+@pytest.mark.parametrize("x_sym,horiz", [(True, True), (True, False), (False, True)])
+def test_visc_apply_equals_accessors(V, x_sym, horiz):
+    torch = _torch()
+    m, n, vfx, vfy = 128, 64, 0.37, 0.41
+    A = vo.visco_matrix(m, n, vfx, vfy, x_sym, horiz)
+    s = V.ViscoImpl(m, n, x_sym, horiz, vfx, vfy)
+    z = np.random.default_rng(3).standard_normal(m * n)
+    s.z.copy_(torch.from_numpy(z))
+    y = s.apply().cpu().numpy()
+    assert _rel(y, A @ z) < 1e-14
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("m,n", [(256, 128), (512, 256)])
+def test_mac_solve_gaussians(V, m, n, prec):
+    torch = _torch()
+    dx = 1. / m
+    b = gaussians_rhs(m, n, seed=7)
+    A = vo.mac_matrix(m, n, 1. / (dx * dx), 1. / (dx * dx))
+    s = V.MgsMac(m, n, dx, dx)
+    s.b.copy_(torch.from_numpy(b))
+    v, rel = s.solve_v_cycle(rtol=1e-10, precision=prec)
+    z = s.z.cpu().numpy()
+    r = b - A @ z
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-10 * (1 + 1e-6)
+    assert rel <= 1e-10
+    assert 1 <= v <= 40
+    zd = vo.DirectSolver(A).solve(b)
+    assert _rel(z, zd) < 1e-6
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_fem_solve(V, prec):
+    torch = _torch()
+    M, N = 257, 129
+    dx = dy = 1. / (M - 1)
+    rng = np.random.default_rng(11)
+    b = np.zeros((N, M))
+    b[1:, :] = gaussians_rhs(M, N - 1, seed=5).reshape(N - 1, M) * dx * dx
+    i = np.arange(M)
+    c = vo.fem_coeffs(dx, dy)
+    b[0, :] = vo.fem_a_cc(M, N, i, 0, c['fm']) * rng.uniform(100, 200, M)
+    b = b.ravel()
+    A = vo.fem_matrix(M, N, dx, dy)
+    s = V.MgsFem(M, N, dx, dy)
+    s.b.copy_(torch.from_numpy(b))
+    v, rel = s.solve_v_cycle(rtol=1e-10, precision=prec)
+    z = s.z.cpu().numpy()
+    assert np.linalg.norm(b - A @ z) / np.linalg.norm(b) <= 1e-10 * (1 + 1e-6)
+    assert v <= 40
+    zd = vo.DirectSolver(A).solve(b)
+    assert _rel(z, zd) < 1e-7
+
+
+@pytest.mark.parametrize("x_sym,horiz", [(True, True), (True, False), (False, False)])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_visc_solve(V, x_sym, horiz, prec):
+    torch = _torch()
+    m, n, vfx, vfy = 256, 128, 0.4, 0.4
+    b = np.random.default_rng(13).standard_normal(m * n)
+    A = vo.visco_matrix(m, n, vfx, vfy, x_sym, horiz)
+    s = V.ViscoImpl(m, n, x_sym, horiz, vfx, vfy)
+    s.b.copy_(torch.from_numpy(b))
+    v, rel = s.solve_v_cycle(rtol=1e-10, precision=prec)
+    z = s.z.cpu().numpy()
+    assert np.linalg.norm(b - A @ z) / np.linalg.norm(b) <= 1e-10 * (1 + 1e-6)
+    assert v <= 20
+    assert _rel(z, vo.DirectSolver(A).solve(b)) < 1e-9
+
+
+def test_zero_rhs_gives_zero(V):
+    torch = _torch()
+    s = V.MgsMac(64, 32, 0.1, 0.1)
+    s.z.fill_(3.0)
+    v, rel = s.solve_v_cycle()
+    assert v == 0 and float(s.z.abs().max()) == 0.0
+
+
+def test_vcycle_cap_reports_error(V):
+    torch = _torch()
+    m, n = 128, 64
+    s = V.MgsMac(m, n, 1. / m, 1. / m)
+    s.b.copy_(torch.from_numpy(gaussians_rhs(m, n, 3)))
+    with pytest.raises(V.VdiError) as e:
+        s.solve_v_cycle(rtol=1e-14, max_vcycles=2)
+    assert e.value.status == 5
+
+
+def test_nonfinite_rhs_reports_error(V):
+    torch = _torch()
+    s = V.MgsMac(64, 32, 0.1, 0.1)
+    s.b.fill_(1.0)
+    s.b[100] = float("nan")
+    with pytest.raises(V.VdiError) as e:
+        s.solve_v_cycle()
+    assert e.value.status == 8
+
+
+def test_matches_reference_dipole_solve(V, ref_driver, tmp_path):
+    """mg_test's dipole source (mg_test.cc:87-91) solved by the reference
+    build and by the GPU, both to a tight tolerance."""
+    import os
+    import subprocess
+    torch = _torch()
+    for kind, m, n in (("mac", 128, 64), ("fem", 129, 65)):
+        dx, dy = 2. / (m - 1), 2. / (n - 1)
+        b = np.zeros(m * n)
+        b[m // 5 + (n // 3) * m] = 1
+        b[(6 * m) // 7 + ((2 * n) // 3) * m] = -1
+        if kind == "fem":
+            b[:m] = 0.
+        bf, zf = tmp_path / "b.bin", tmp_path / "z.bin"
+        b.tofile(bf)
+        env = dict(os.environ, VDI_MG_RTOL="1e-13")
+        subprocess.run([ref_driver, kind, str(m), str(n), repr(dx), repr(dy), str(bf), str(zf)], check=True,
+                       env=env, capture_output=True)
+        zr = np.fromfile(zf)
+        s = (V.MgsMac if kind == "mac" else V.MgsFem)(m, n, dx, dy)
+        s.b.copy_(torch.from_numpy(b))
+        s.solve_v_cycle(rtol=1e-13)
+        assert _rel(s.z.cpu().numpy(), zr) < 1e-9, kind

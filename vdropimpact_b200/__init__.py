@@ -1,0 +1,310 @@
+"""B200 implementation of vdropimpact's per-timestep fluid solve.
+
+Python host-side mirror of the reference's classes, over the C ABI of
+include/vdi.h (libvdi.so):
+
+    Fluid2D      fluid_2d      (fluid_2d.hh:21-142): init_fields,
+                 step_forward, timestep_select, solve, restart-style state
+    MgsMac       mgs_mac       (mgs_mac.hh:25-75)  : solve_v_cycle, v_cycle
+    MgsFem       mgs_fem       (mgs_fem.hh:36-82)  : solve_v_cycle, v_cycle
+    ViscoImpl    visco_impl    (visco_impl.hh:17-58): setup_and_solve
+    TriSolve     tri_solve     (tri_solve.hh:6-22) : solve_lapack
+
+Errors the reference reports with fatal_error()/exit() raise VdiError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import (VDI_MG_FP64, VDI_MG_MIXED, VDI_GUESS_EXTRAPOLATE, VDI_GUESS_LEARNED, VDI_MG_MAC,
+                   VDI_MG_FEM, VDI_MG_VISC_U, VDI_MG_VISC_V, VdiError, check, lib)
+
+__all__ = ["Fluid2D", "MgsMac", "MgsFem", "ViscoImpl", "TriSolve", "VdiError", "params_from_cfg",
+           "VDI_MG_FP64", "VDI_MG_MIXED", "VDI_GUESS_EXTRAPOLATE", "VDI_GUESS_LEARNED"]
+
+_PREC = {"fp64": VDI_MG_FP64, "mixed": VDI_MG_MIXED, VDI_MG_FP64: VDI_MG_FP64, VDI_MG_MIXED: VDI_MG_MIXED}
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("vdropimpact_b200 needs a CUDA device")
+    return torch
+
+
+def _stream_handle(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+def params_from_cfg(cfg: str) -> _abi.VdiParams:
+    """fileinfo::fileinfo (fileinfo.cc:11-193) for a path ending in .cfg or
+    for configuration text."""
+    text = open(cfg).read() if (cfg.endswith(".cfg") and os.path.exists(cfg)) else cfg
+    p = _abi.VdiParams()
+    check(lib().vdi_params_from_cfg(text.encode(), C.byref(p)), "vdi_params_from_cfg")
+    return p
+
+
+class Fluid2D:
+    """fluid_2d (fluid_2d.hh:21-142) on the GPU."""
+
+    def __init__(self, cfg, *, mg_rtol: float = 1e-10, mg_max_vcycles: int = 200,
+                 mg_precision="fp64", graph: bool = False, stream=None):
+        self.prm = cfg if isinstance(cfg, _abi.VdiParams) else params_from_cfg(cfg)
+        self.prm.mg_rtol = mg_rtol
+        self.prm.mg_max_vcycles = mg_max_vcycles
+        self.prm.mg_precision = _PREC[mg_precision]
+        self.m, self.n = self.prm.m, self.prm.n
+        self.me, self.ne, self.ml = self.m + 1, self.n + 1, self.m + 4
+        self.dx = (self.prm.bx - self.prm.ax) / self.m
+        self.dy = (self.prm.by - self.prm.ay) / self.n
+        h = C.c_void_p()
+        check(lib().vdi_sim_create(C.byref(self.prm), _stream_handle(stream), C.byref(h)), "vdi_sim_create")
+        self._h = h
+        if graph:
+            self.use_graph(True)
+
+    # ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vdi_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------
+    def init_fields(self):
+        """fluid_2d::init_fields (fluid_2d_sio.cc:14-35)."""
+        check(lib().vdi_sim_init_fields(self._h), "vdi_sim_init_fields")
+
+    def timestep_select(self, interval: float):
+        """fluid_2d::timestep_select (fluid_2d.hh:82-86): returns (l, adt)."""
+        adt = C.c_double()
+        l = C.c_int()
+        check(lib().vdi_sim_timestep_select(self._h, interval, C.byref(adt), C.byref(l)), "timestep_select")
+        return l.value, adt.value
+
+    def frame_dt(self) -> float:
+        """The timestep of fluid_2d::solve (fluid_2d.cc:42)."""
+        return self.timestep_select(self.prm.t_end / self.prm.nframes)[1]
+
+    def step_forward(self, dt: float, nsteps: int = 1):
+        """fluid_2d::step_forward (fluid_2d.cc:93-405), nsteps times."""
+        check(lib().vdi_sim_step_forward(self._h, dt, nsteps), "vdi_sim_step_forward")
+
+    def use_graph(self, enable: bool = True):
+        check(lib().vdi_sim_use_graph(self._h, int(enable)), "vdi_sim_use_graph")
+
+    def synchronize(self):
+        check(lib().vdi_sim_synchronize(self._h), "vdi_sim_synchronize")
+
+    def solve(self, frames: int | None = None, callback=None):
+        """fluid_2d::solve (fluid_2d.cc:40-89) without file output: steps
+        `frames` frames of l steps each and calls callback(k, self)."""
+        l, adt = self.timestep_select(self.prm.t_end / self.prm.nframes)
+        for k in range(1, (frames or self.prm.nframes) + 1):
+            self.step_forward(adt, l)
+            if callback:
+                callback(k, self)
+
+    # ------------------------------------------------------------------
+    def _arrays(self):
+        m, n = self.m, self.n
+        ng = (m + 4) * (n + 4)
+        return dict(u=np.zeros(ng), v=np.zeros(ng), p=np.zeros(ng), gp=np.zeros(m + 1),
+                    tau=np.zeros(m + 4), h=np.zeros(m), fbd=np.zeros(m), pg=np.zeros(m + 1), ht=np.zeros(m))
+
+    @staticmethod
+    def _ptr(a):
+        return a.ctypes.data_as(_abi._dp)
+
+    def state(self) -> dict:
+        """The restart-file state (fluid_2d_sio.cc:97-119,
+        gas_layer_solve.cc:323-329) as numpy arrays; u, v, p have shape
+        (n+4, m+4)."""
+        a = self._arrays()
+        st = _abi.VdiState()
+        for k, v in a.items():
+            setattr(st, k, self._ptr(v))
+        check(lib().vdi_sim_get_state(self._h, C.byref(st)), "vdi_sim_get_state")
+        shp = (self.n + 4, self.m + 4)
+        out = dict(m=self.m, n=self.n, time=st.time, Vframe=st.Vframe)
+        for k, v in a.items():
+            out[k] = v.reshape(shp) if k in ("u", "v", "p") else v
+        return out
+
+    def load(self, s: dict):
+        """Loads a state (the restart loader, fluid_2d_sio.cc:39-62); the
+        multigrid time-extrapolation history restarts as in the reference."""
+        keep = {}
+        st = _abi.VdiState()
+        st.time = float(s["time"])
+        st.Vframe = float(s["Vframe"])
+        for k in ("u", "v", "p", "gp", "tau", "h", "fbd", "pg", "ht"):
+            a = np.ascontiguousarray(s[k], dtype=np.float64).ravel()
+            keep[k] = a
+            setattr(st, k, self._ptr(a))
+        check(lib().vdi_sim_set_state(self._h, C.byref(st)), "vdi_sim_set_state")
+
+    def stats(self, reset: bool = False) -> dict:
+        s = _abi.VdiStats()
+        check(lib().vdi_sim_stats(self._h, C.byref(s), int(reset)), "vdi_sim_stats")
+        names = ("MAC", "FEM", "VX", "VY")
+        return dict(steps=s.steps, solves=dict(zip(names, list(s.solves))),
+                    vcycles=dict(zip(names, list(s.vcycles))), newton_steps=s.newton_steps,
+                    tri_pivot_fallbacks=s.tri_pivot_fallbacks,
+                    height_fixed_point_iters=s.height_fixed_point_iters,
+                    last_rel_res=dict(zip(names, list(s.last_rel_res))))
+
+    def device_field(self, which: int):
+        p = _abi._dp()
+        n = C.c_size_t()
+        check(lib().vdi_sim_device_field(self._h, which, C.byref(p), C.byref(n)), "vdi_sim_device_field")
+        return C.cast(p, C.c_void_p).value, n.value
+
+
+class _MgSystem:
+    """Common part of the TGMG-style problem classes: a device solution z and
+    source b (torch float64 tensors on the current CUDA device) and the
+    solver calls of tgmg (mg_test.cc:20-45)."""
+
+    kind = None
+    precision = "fp64"
+
+    def __init__(self, m, n, c1, c2, x_sym=False, stream=None):
+        torch = _torch()
+        self.m, self.n, self.mn = m, n, m * n
+        self.z = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        self.b = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        self._stream = stream
+        h = C.c_void_p()
+        check(lib().vdi_mg_create(self.kind, m, n, c1, c2, int(x_sym), _stream_handle(stream), C.byref(h)),
+              "vdi_mg_create")
+        self._h = h
+        self.last = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                lib().vdi_mg_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def setup(self):
+        check(lib().vdi_mg_setup(self._h), "vdi_mg_setup")
+
+    def solve_v_cycle(self, rtol: float = 1e-10, max_vcycles: int = 200, precision=None):
+        """tgmg::solve_v_cycle: V-cycles on z from its current value until
+        ||b-Az||/||b|| <= rtol. Returns (vcycles, relative residual)."""
+        _torch().cuda.synchronize()
+        r = _abi.VdiMgResult()
+        check(lib().vdi_mg_solve(self._h, C.c_void_p(self.b.data_ptr()), C.c_void_p(self.z.data_ptr()),
+                                 rtol, max_vcycles, _PREC[precision or self.precision], C.byref(r)),
+              "vdi_mg_solve")
+        self.last = (r.vcycles, r.rel_res)
+        return self.last
+
+    def v_cycle(self):
+        """tgmg::v_cycle: one FP64 V-cycle on z."""
+        _torch().cuda.synchronize()
+        check(lib().vdi_mg_v_cycle(self._h, C.c_void_p(self.b.data_ptr()), C.c_void_p(self.z.data_ptr())),
+              "vdi_mg_v_cycle")
+
+    def apply(self, z=None):
+        """A z (a_cc*z + mul_a of the problem class)."""
+        torch = _torch()
+        z = self.z if z is None else z
+        y = torch.empty_like(z)
+        torch.cuda.synchronize()
+        check(lib().vdi_mg_apply(self._h, C.c_void_p(z.data_ptr()), C.c_void_p(y.data_ptr())), "vdi_mg_apply")
+        return y
+
+    def residual(self):
+        """(r, ||r||_2) with r = b - A z (tgmg::output_res)."""
+        torch = _torch()
+        r = torch.empty_like(self.z)
+        nrm = C.c_double()
+        torch.cuda.synchronize()
+        check(lib().vdi_mg_residual(self._h, C.c_void_p(self.b.data_ptr()), C.c_void_p(self.z.data_ptr()),
+                                    C.c_void_p(r.data_ptr()), C.byref(nrm)), "vdi_mg_residual")
+        return r, nrm.value
+
+
+class MgsMac(_MgSystem):
+    """mgs_mac(int m,int n,double dx,double dy,double* b) (mgs_mac.cc:23-27)."""
+    kind = VDI_MG_MAC
+
+    def __init__(self, m, n, dx, dy, stream=None):
+        super().__init__(m, n, dx, dy, False, stream)
+
+
+class MgsFem(_MgSystem):
+    """mgs_fem(int m,int n,double dx,double dy,double* b) (mgs_fem.cc:26-30);
+    m x n nodes."""
+    kind = VDI_MG_FEM
+
+    def __init__(self, m, n, dx, dy, stream=None):
+        super().__init__(m, n, dx, dy, False, stream)
+
+
+class ViscoImpl(_MgSystem):
+    """visco_impl (visco_impl.hh:17-58) on an m x n grid."""
+
+    def __init__(self, m, n, x_sym: bool, horizontal_vel: bool, vfx=1., vfy=1., stream=None):
+        self.kind = VDI_MG_VISC_U if horizontal_vel else VDI_MG_VISC_V
+        self.x_sym, self.horizontal_vel = x_sym, horizontal_vel
+        self.vfx, self.vfy = vfx, vfy
+        super().__init__(m, n, vfx, vfy, x_sym, stream)
+
+    def setup_and_solve(self, vfx, vfy, rtol=1e-10, max_vcycles=200, precision=None):
+        """visco_impl::setup_and_solve (visco_impl.cc:21-39) without the time
+        extrapolation (the caller supplies z)."""
+        if abs(vfx - self.vfx) > 1e2 * np.finfo(float).eps * self.vfx or vfy != self.vfy:
+            h = C.c_void_p()
+            check(lib().vdi_mg_create(self.kind, self.m, self.n, vfx, vfy, int(self.x_sym),
+                                      _stream_handle(self._stream), C.byref(h)), "vdi_mg_create")
+            lib().vdi_mg_destroy(self._h)
+            self._h = h
+            self.vfx, self.vfy = vfx, vfy
+        return self.solve_v_cycle(rtol, max_vcycles, precision)
+
+
+class TriSolve:
+    """tri_solve (tri_solve.hh:6-22): host arrays a, b, c, d of length m;
+    solve_lapack() solves on the GPU and leaves the solution in d."""
+
+    def __init__(self, m: int):
+        self.m = m
+        self.a = np.zeros(m)
+        self.b = np.zeros(m)
+        self.c = np.zeros(m)
+        self.d = np.zeros(m)
+        self.pivoted = False
+
+    def solve_lapack(self):
+        torch = _torch()
+        dev = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (self.a, self.b, self.c, self.d)]
+        piv = C.c_int()
+        torch.cuda.synchronize()
+        check(lib().vdi_tri_solve(self.m, *[C.c_void_p(t.data_ptr()) for t in dev], None, C.byref(piv)),
+              "vdi_tri_solve")
+        self.d = dev[3].cpu().numpy()
+        self.pivoted = bool(piv.value)
+        return self.d

@@ -1,0 +1,74 @@
+"""Builds libvdi.so (the CUDA kernels and the C ABI of include/vdi.h) for
+sm_100a with nvcc, in the package tree, so it travels with the sources.
+
+    python -m vdropimpact_b200.build [--force]
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(OUT_DIR, "libvdi.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
+                 "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+# Stencil and gas-layer kernels follow the reference's expression order
+# exactly; FMA contraction would change their rounding.
+EXACT = {"step_kernels.cu", "gas.cu"}
+SOURCES = ["mg.cu", "step_kernels.cu", "gas.cu", "sim.cu", "unet.cu", "batch.cu", "host_api.cu"]
+
+
+def _sources():
+    return [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+
+
+def _deps():
+    hdrs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".hh", ".cuh", ".h"))]
+    hdrs.append(os.path.join(ROOT, "include", "vdi.h"))
+    return hdrs
+
+
+def _compile(src: str) -> str:
+    obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
+    path = os.path.join(CSRC, src)
+    newest = max([os.path.getmtime(path)] + [os.path.getmtime(h) for h in _deps()])
+    if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
+        return obj
+    flags = COMMON + (["-fmad=false"] if src in EXACT else [])
+    cmd = [NVCC] + flags + ["-c", path, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(OUT_DIR, exist_ok=True)
+    if force:
+        for f in os.listdir(OUT_DIR):
+            if f.endswith((".o", ".so")):
+                os.remove(os.path.join(OUT_DIR, f))
+    srcs = _sources()
+    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+        objs = list(ex.map(_compile, srcs))
+    newest = max(os.path.getmtime(o) for o in objs)
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        print(LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

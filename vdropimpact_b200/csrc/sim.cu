@@ -1,0 +1,661 @@
+// The step driver (fluid_2d, fluid_2d.cc:14-405) over the device kernels,
+// and the C ABI declared in include/vdi.h.
+#include "step_kernels.hh"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace vdi {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+}  // namespace vdi
+
+using namespace vdi;
+
+enum { SOLVER_MAC = 0, SOLVER_FEM = 1, SOLVER_VX = 2, SOLVER_VY = 3 };
+
+struct vdi_sim {
+    vdi_params prm{};
+    Grid g{};
+    GasPrm gp{};
+    double dt_reg = 0;
+    cudaStream_t s = nullptr, s_gas = nullptr, s_vy = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev_fork = nullptr, ev_gas = nullptr, ev_vy = nullptr, ev_vy_done = nullptr;
+    std::vector<double*> bufs;
+    Fields f{};
+    Gas gas{};
+    double* gas_work = nullptr;
+    double *src_mac = nullptr, *q = nullptr, *q_prev = nullptr;
+    double *src_fem = nullptr, *zf = nullptr, *zf_prev = nullptr;
+    double *su = nullptr, *sv = nullptr, *zu = nullptr, *zu_prev = nullptr, *zv = nullptr, *zv_prev = nullptr;
+    GuessHist* hist = nullptr;   // 4 entries
+    double* d_time = nullptr;
+    double* d_vframe = nullptr;
+    int* d_err = nullptr;
+    GasStats* d_gstats = nullptr;
+    MG* mg[4] = {nullptr, nullptr, nullptr, nullptr};
+    double vfx_cur = 0, vfy_cur = 0;
+    double fem_acc_edge = 0, fem_acc_mid = 0;
+    // graph replay of one step
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    double graph_dt = 0;
+    long steps = 0;
+};
+
+namespace {
+
+int alloc_zero(vdi_sim* S, double** p, size_t n) {
+    VDI_CUDA(cudaMalloc(p, n * sizeof(double)));
+    VDI_CUDA(cudaMemset(*p, 0, n * sizeof(double)));
+    S->bufs.push_back(*p);
+    return VDI_OK;
+}
+
+size_t ghosted(const vdi_sim* S) { return size_t(S->prm.m + 4) * (S->prm.n + 4); }
+
+/** visco_impl::setup_and_solve's re-setup test (visco_impl.cc:26-30). */
+int update_visc(vdi_sim* S, double dt) {
+    const Grid& g = S->g;
+    if (!g.implicit_visc) return VDI_OK;
+    double vfx = g.viscfac * g.xxsp * dt, vfy = g.viscfac * g.yysp * dt;
+    if (std::fabs(vfx - S->vfx_cur) > 1e2 * 2.220446049250313e-16 * S->vfx_cur || S->vfx_cur == 0) {
+        S->vfx_cur = vfx;
+        S->vfy_cur = vfy;
+        VDI_TRY(mg_set_visc(S->mg[SOLVER_VX], vfx, vfy));
+        VDI_TRY(mg_set_visc(S->mg[SOLVER_VY], vfx, vfy));
+    }
+    return VDI_OK;
+}
+
+/** Enqueues one fluid_2d::step_forward(dt) (fluid_2d.cc:93-405). */
+int enqueue_step(vdi_sim* S, double dt) {
+    const Grid& g = S->g;
+    cudaStream_t s = S->s;
+    const int m = g.m, n = g.n, mn = m * n, nf = (m + 1) * (n + 1);
+    int prec = S->prm.mg_precision;
+    // gas layer on its own stream; it overlaps the advection stages
+    VDI_CUDA(cudaEventRecord(S->ev_fork, s));
+    VDI_CUDA(cudaStreamWaitEvent(S->s_gas, S->ev_fork, 0));
+    VDI_TRY(launch_gas_update(S->s_gas, S->gp, S->gas, S->f.u, S->f.v, m + 4, S->d_vframe, dt, S->d_time,
+                              S->gas_work, S->d_err, S->d_gstats));
+    VDI_CUDA(cudaEventRecord(S->ev_gas, S->s_gas));
+    VDI_TRY(launch_stage1(s, g, S->f, dt));
+    VDI_TRY(launch_stage2(s, g, S->f));
+    VDI_TRY(launch_stage34(s, g, S->f, dt));
+    VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
+    VDI_TRY(launch_stage5_src(s, g, S->f, S->gas, dt, S->src_mac));
+    VDI_TRY(launch_guess(s, S->q, S->q_prev, mn, S->hist + SOLVER_MAC, S->d_time, S->d_err));
+    VDI_TRY(mg_solve_device(S->mg[SOLVER_MAC], s, S->src_mac, S->q, prec));
+    VDI_TRY(launch_mac_advect(s, g, S->f, S->gas, S->q, dt, S->d_time));
+    VDI_TRY(launch_inviscid_bc(s, g, S->f, S->gas, dt));
+    VDI_TRY(launch_viscous_bc(s, g, S->f, S->gas));
+    CellView c0v, c1v;
+    if (g.implicit_visc) {
+        VDI_TRY(launch_visc_rhs(s, g, S->f, S->gas, S->vfx_cur, S->vfy_cur, S->su, S->sv));
+        cudaStreamCaptureStatus cs;
+        VDI_CUDA(cudaStreamIsCapturing(s, &cs));
+        bool par = cs == cudaStreamCaptureStatusActive;
+        cudaStream_t sv = par ? S->s_vy : s;
+        if (par) {
+            VDI_CUDA(cudaEventRecord(S->ev_vy, s));
+            VDI_CUDA(cudaStreamWaitEvent(S->s_vy, S->ev_vy, 0));
+        }
+        VDI_TRY(launch_guess(s, S->zu, S->zu_prev, mn, S->hist + SOLVER_VX, S->d_time, S->d_err));
+        VDI_TRY(mg_solve_device(S->mg[SOLVER_VX], s, S->su, S->zu, prec));
+        VDI_TRY(launch_guess(sv, S->zv, S->zv_prev, mn, S->hist + SOLVER_VY, S->d_time, S->d_err));
+        VDI_TRY(mg_solve_device(S->mg[SOLVER_VY], sv, S->sv, S->zv, prec));
+        if (par) {
+            VDI_CUDA(cudaEventRecord(S->ev_vy_done, S->s_vy));
+            VDI_CUDA(cudaStreamWaitEvent(s, S->ev_vy_done, 0));
+        }
+        c0v = CellView{S->zu, m, 0};
+        c1v = CellView{S->zv, m, 0};
+    } else {
+        c0v = CellView{S->f.fc0, m + 4, 2 * (m + 4) + 2};
+        c1v = CellView{S->f.fc1, m + 4, 2 * (m + 4) + 2};
+    }
+    VDI_TRY(launch_fem_rhs(s, g, S->f, S->gas, c0v, c1v, dt, S->fem_acc_edge, S->fem_acc_mid, S->src_fem));
+    VDI_TRY(launch_guess(s, S->zf, S->zf_prev, nf, S->hist + SOLVER_FEM, S->d_time, S->d_err));
+    VDI_TRY(mg_solve_device(S->mg[SOLVER_FEM], s, S->src_fem, S->zf, prec));
+    VDI_TRY(launch_vel_update(s, g, S->f, c0v, c1v, S->zf, dt));
+    VDI_TRY(launch_viscous_bc(s, g, S->f, S->gas));
+    return VDI_OK;
+}
+
+int check_errors(vdi_sim* S) {
+    int err = 0;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    VDI_CUDA(cudaMemcpy(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 4; k++) {
+        if (!S->mg[k]) continue;
+        SolveCtl c;
+        VDI_CUDA(cudaMemcpy(&c, mg_ctl(S->mg[k]), sizeof(SolveCtl), cudaMemcpyDeviceToHost));
+        err |= c.sticky;
+    }
+    if (err & DEV_NONFINITE) {
+        set_error("non-finite value in a residual");
+        return VDI_ERR_NONFINITE;
+    }
+    if (err & DEV_MG_NOT_CONVERGED) {
+        set_error("a multigrid solve reached its V-cycle cap");
+        return VDI_ERR_MG_NOT_CONVERGED;
+    }
+    if (err & DEV_NEWTON) {
+        set_error("gas layer: too many Newton steps");
+        return VDI_ERR_NEWTON_NOT_CONVERGED;
+    }
+    if (err & DEV_TRI_SINGULAR) {
+        set_error("gas layer: singular tridiagonal system");
+        return VDI_ERR_TRI_SINGULAR;
+    }
+    return VDI_OK;
+}
+
+void destroy_graph(vdi_sim* S) {
+    if (S->gexec) cudaGraphExecDestroy(S->gexec);
+    if (S->graph) cudaGraphDestroy(S->graph);
+    S->gexec = nullptr;
+    S->graph = nullptr;
+}
+
+int capture_step(vdi_sim* S, double dt) {
+    destroy_graph(S);
+    VDI_TRY(update_visc(S, dt));
+    VDI_CUDA(cudaStreamBeginCapture(S->s, cudaStreamCaptureModeRelaxed));
+    int st = enqueue_step(S, dt);
+    cudaGraph_t gph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(S->s, &gph);
+    if (st != VDI_OK) {
+        if (gph) cudaGraphDestroy(gph);
+        return st;
+    }
+    VDI_CUDA(e);
+    S->graph = gph;
+    VDI_CUDA(cudaGraphInstantiate(&S->gexec, gph, 0));
+    S->graph_dt = dt;
+    return VDI_OK;
+}
+
+int parse_cfg(const char* text, vdi_params* P) {
+    // fileinfo.cc:11-193 for the gas_layer_model path
+    int m = -1, n = -1, nframes = -1, glo = 0;
+    double L_nd = -1, h0_nd = -1, t_end_nd = -1, tmult = -1, nul = -1, rho = -1, R = -1, V = -1, alpha = -1,
+           sigma = -1, mug = -1, Pamb = -1;
+    int x_sym = 0, implicit_visc = 0;
+    std::istringstream in(text);
+    std::string line;
+    int ln = 0;
+    while (std::getline(in, line)) {
+        ln++;
+        size_t h = line.find('#');
+        if (h != std::string::npos) line = line.substr(0, h);
+        std::istringstream ls(line);
+        std::string key;
+        if (!(ls >> key)) continue;
+        std::vector<std::string> vals;
+        std::string t;
+        while (ls >> t) vals.push_back(t);
+        auto num = [&](size_t k) -> double {
+            if (k >= vals.size()) return std::nan("");
+            return atof(vals[k].c_str());
+        };
+        if (key == "grid_points") {
+            if (vals.size() != 2) { set_error("grid_points needs two values (line %d)", ln); return VDI_ERR_CONFIG; }
+            m = atoi(vals[0].c_str()); n = atoi(vals[1].c_str());
+        } else if (key == "L_nd") L_nd = num(0);
+        else if (key == "h0_nd") h0_nd = num(0);
+        else if (key == "t_end_nd") t_end_nd = num(0);
+        else if (key == "frames") nframes = int(num(0));
+        else if (key == "tmult") tmult = num(0);
+        else if (key == "nul") nul = num(0);
+        else if (key == "nul_cSt") nul = 1e-6 * num(0);
+        else if (key == "rhol") rho = num(0);
+        else if (key == "R") R = num(0);
+        else if (key == "V") V = num(0);
+        else if (key == "gamma") alpha = 1. / num(0);
+        else if (key == "alpha") alpha = num(0);
+        else if (key == "sigma") sigma = num(0);
+        else if (key == "mug") mug = num(0);
+        else if (key == "Pamb") Pamb = num(0);
+        else if (key == "x_sym") x_sym = 1;
+        else if (key == "implicit_visc") implicit_visc = 1;
+        else if (key == "gas_layer_model") glo = 2;
+        else if (key == "mr_time_output" || key == "tracers" || key == "restart_freq" || key == "output") {
+        } else if (key == "gas_layer_data" || key == "nif_center" || key == "nif_range") {
+            set_error("option '%s' is outside the GPU path (line %d)", key.c_str(), ln);
+            return VDI_ERR_CONFIG;
+        } else {
+            set_error("Keyword '%s' not understood on line %d", key.c_str(), ln);
+            return VDI_ERR_CONFIG;
+        }
+    }
+    if (m <= 0 || n <= 0) { set_error("Grid dimensions not set"); return VDI_ERR_CONFIG; }
+    const char* names[] = {"L_nd", "h0_nd", "t_end_nd", "tmult", "frames", "nul", "rhol",
+                           "alpha", "mug", "Pamb", "R", "V", "sigma"};
+    double vals[] = {L_nd, h0_nd, t_end_nd, tmult, double(nframes), nul, rho, alpha, mug, Pamb, R, V, sigma};
+    for (int k = 0; k < 13; k++)
+        if (!(vals[k] >= 0)) { set_error("Value of %s either invalid or not set", names[k]); return VDI_ERR_CONFIG; }
+    if (glo != 2) { set_error("gas_layer_model must be set"); return VDI_ERR_CONFIG; }
+    memset(P, 0, sizeof(*P));
+    P->m = m; P->n = n; P->x_sym = x_sym; P->implicit_visc = implicit_visc;
+    P->rho = rho;
+    P->mu = nul * rho;                                  // fileinfo.cc:143
+    double st = mug / (rho * V * R), st3 = pow(st, 1. / 3.), st23 = st3 * st3;
+    double L = L_nd * R * st3;
+    P->h0 = h0_nd * R * st23;
+    P->t_end = t_end_nd * R * st23 / V;
+    P->bx = L; P->by = L * n / m; P->ay = 0;
+    if (x_sym) P->ax = 0;
+    else { P->ax = -L; P->by *= 2; }
+    P->tmult = tmult; P->nframes = nframes;
+    P->alpha = alpha; P->mug = mug; P->Pamb = Pamb; P->R = R; P->V = V; P->sigma = sigma;
+    P->mg_rtol = 1e-10;
+    P->mg_max_vcycles = 200;
+    P->mg_precision = VDI_MG_FP64;
+    P->mg_guess = VDI_GUESS_EXTRAPOLATE;
+    return VDI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vdi_status_string(int s) {
+    switch (s) {
+        case VDI_OK: return "ok";
+        case VDI_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case VDI_ERR_UNSUPPORTED_SIZE: return "unsupported grid size";
+        case VDI_ERR_CUDA: return "CUDA error";
+        case VDI_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case VDI_ERR_MG_NOT_CONVERGED: return "multigrid did not converge";
+        case VDI_ERR_NEWTON_NOT_CONVERGED: return "Newton iteration did not converge";
+        case VDI_ERR_TRI_SINGULAR: return "singular tridiagonal system";
+        case VDI_ERR_NONFINITE: return "non-finite value";
+        case VDI_ERR_CONFIG: return "configuration error";
+        case VDI_ERR_NOT_READY: return "not ready";
+    }
+    return "unknown status";
+}
+
+int vdi_abi_version(void) { return VDI_ABI_VERSION; }
+const char* vdi_last_error(void) { return g_err; }
+
+int vdi_params_from_cfg(const char* cfg_text, vdi_params* out) {
+    if (!cfg_text || !out) return VDI_ERR_INVALID_ARGUMENT;
+    return parse_cfg(cfg_text, out);
+}
+
+int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
+    if (!prm || !out || prm->m < 4 || prm->n < 4) {
+        set_error("vdi_sim_create: invalid parameters");
+        return VDI_ERR_INVALID_ARGUMENT;
+    }
+    vdi_sim* S = new vdi_sim();
+    S->prm = *prm;
+    if (S->prm.mg_rtol <= 0) S->prm.mg_rtol = 1e-10;
+    if (S->prm.mg_max_vcycles <= 0) S->prm.mg_max_vcycles = 200;
+    Grid& g = S->g;
+    const vdi_params& P = S->prm;
+    g.m = P.m; g.n = P.n; g.x_sym = P.x_sym; g.implicit_visc = P.implicit_visc;
+    g.ax = P.ax; g.ay = P.ay; g.bx = P.bx; g.by = P.by;
+    // fluid_2d.cc:15-17
+    g.dx = (P.bx - P.ax) / P.m;
+    g.dy = (P.by - P.ay) / P.n;
+    g.xsp = 1. / g.dx; g.ysp = 1. / g.dy;
+    g.xxsp = g.xsp * g.xsp; g.yysp = g.ysp * g.ysp;
+    g.rho = P.rho; g.rhoinv = 1. / P.rho; g.mu = P.mu; g.muinv = 1. / P.mu;
+    g.viscfac = P.implicit_visc ? g.rhoinv * g.mu * 0.5 : g.rhoinv * g.mu;   // fluid_2d.cc:164
+    S->dt_reg = P.implicit_visc ? g.dx * P.tmult : g.dx * g.dx * P.rho * g.muinv * P.tmult * 0.25;
+    GasPrm& gp = S->gp;
+    gp.m = P.m; gp.x_sym = P.x_sym; gp.ax = P.ax;
+    gp.dx = (P.bx - P.ax) / P.m;       // gas_layer.cc:9
+    gp.xsp = 1. / gp.dx; gp.xxsp = gp.xsp * gp.xsp;
+    gp.alpha = P.alpha; gp.mu = P.mug; gp.Pamb = P.Pamb; gp.R = P.R; gp.sigma = P.sigma;
+
+    auto fail = [&](int st) {
+        vdi_sim_destroy(S);
+        return st;
+    };
+    int st;
+    if (stream) {
+        S->s = static_cast<cudaStream_t>(stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&S->s, cudaStreamNonBlocking) != cudaSuccess) return fail(VDI_ERR_CUDA);
+        S->own_stream = true;
+    }
+    if (cudaStreamCreateWithFlags(&S->s_gas, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&S->s_vy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_gas, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_vy, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_vy_done, cudaEventDisableTiming) != cudaSuccess)
+        return fail(VDI_ERR_CUDA);
+    size_t NG = ghosted(S);
+    double** fptrs[] = {&S->f.u, &S->f.v, &S->f.p, &S->f.ux, &S->f.uy, &S->f.vx, &S->f.vy,
+                        &S->f.ud, &S->f.vd, &S->f.ul, &S->f.vl, &S->f.ur, &S->f.vr, &S->f.uu, &S->f.vu,
+                        &S->f.ud2, &S->f.vd2, &S->f.ul2, &S->f.vl2, &S->f.ur2, &S->f.vr2, &S->f.uu2, &S->f.vu2,
+                        &S->f.fc0, &S->f.fc1};
+    for (auto pp : fptrs)
+        if ((st = alloc_zero(S, pp, NG)) != VDI_OK) return fail(st);
+    const int m = P.m, n = P.n;
+    size_t mn = size_t(m) * n, nf = size_t(m + 1) * (n + 1);
+    double** gptrs[] = {&S->gas.gp, &S->gas.gp_old, &S->gas.pg, &S->gas.pg_old, &S->gas.hx};
+    for (auto pp : gptrs)
+        if ((st = alloc_zero(S, pp, m + 1)) != VDI_OK) return fail(st);
+    double** gptrs2[] = {&S->gas.tau, &S->gas.tau_old};
+    for (auto pp : gptrs2)
+        if ((st = alloc_zero(S, pp, m + 4)) != VDI_OK) return fail(st);
+    double** gptrs3[] = {&S->gas.h, &S->gas.ht, &S->gas.fbd};
+    for (auto pp : gptrs3)
+        if ((st = alloc_zero(S, pp, m)) != VDI_OK) return fail(st);
+    if ((st = alloc_zero(S, &S->gas_work, gas_work_doubles(m))) != VDI_OK) return fail(st);
+    double** cells[] = {&S->src_mac, &S->q, &S->q_prev, &S->su, &S->sv, &S->zu, &S->zu_prev, &S->zv, &S->zv_prev};
+    for (auto pp : cells)
+        if ((st = alloc_zero(S, pp, mn)) != VDI_OK) return fail(st);
+    double** nodes[] = {&S->src_fem, &S->zf, &S->zf_prev};
+    for (auto pp : nodes)
+        if ((st = alloc_zero(S, pp, nf)) != VDI_OK) return fail(st);
+    double* misc;
+    if ((st = alloc_zero(S, &misc, 2 + 4 * 4)) != VDI_OK) return fail(st);
+    S->d_time = misc;
+    S->d_vframe = misc + 1;
+    S->hist = reinterpret_cast<GuessHist*>(misc + 2);
+    double* ebuf;
+    if ((st = alloc_zero(S, &ebuf, 1 + sizeof(GasStats) / 8 + 1)) != VDI_OK) return fail(st);
+    S->d_err = reinterpret_cast<int*>(ebuf);
+    S->d_gstats = reinterpret_cast<GasStats*>(ebuf + 1);
+    // the four linear systems (fluid_2d.cc:19-21)
+    if ((st = mg_create(VDI_MG_MAC, m, n, g.xxsp, g.yysp, P.x_sym, &S->mg[SOLVER_MAC])) != VDI_OK) return fail(st);
+    if ((st = mg_create(VDI_MG_FEM, m + 1, n + 1, g.dx, g.dy, P.x_sym, &S->mg[SOLVER_FEM])) != VDI_OK)
+        return fail(st);
+    if (P.implicit_visc) {
+        if ((st = mg_create(VDI_MG_VISC_U, m, n, 1., 1., P.x_sym, &S->mg[SOLVER_VX])) != VDI_OK) return fail(st);
+        if ((st = mg_create(VDI_MG_VISC_V, m, n, 1., 1., P.x_sym, &S->mg[SOLVER_VY])) != VDI_OK) return fail(st);
+    }
+    for (int k = 0; k < 4; k++)
+        if (S->mg[k] && (st = mg_configure(S->mg[k], S->prm.mg_rtol, S->prm.mg_max_vcycles)) != VDI_OK)
+            return fail(st);
+    // mgs_fem::a_cc on the bottom row (mgs_fem.hh:55-57)
+    double dydx = g.dy / g.dx, dxdy = g.dx / g.dy, fm = 4. / 3. * (dxdy + dydx);
+    S->fem_acc_edge = 0.5 * 0.5 * fm;
+    S->fem_acc_mid = 1. * 0.5 * fm;
+    *out = S;
+    return VDI_OK;
+}
+
+int vdi_sim_destroy(vdi_sim* S) {
+    if (!S) return VDI_OK;
+    if (S->s) cudaStreamSynchronize(S->s);
+    destroy_graph(S);
+    for (int k = 0; k < 4; k++)
+        if (S->mg[k]) mg_destroy(S->mg[k]);
+    for (auto p : S->bufs) cudaFree(p);
+    if (S->ev_fork) cudaEventDestroy(S->ev_fork);
+    if (S->ev_gas) cudaEventDestroy(S->ev_gas);
+    if (S->ev_vy) cudaEventDestroy(S->ev_vy);
+    if (S->ev_vy_done) cudaEventDestroy(S->ev_vy_done);
+    if (S->s_gas) cudaStreamDestroy(S->s_gas);
+    if (S->s_vy) cudaStreamDestroy(S->s_vy);
+    if (S->own_stream && S->s) cudaStreamDestroy(S->s);
+    delete S;
+    return VDI_OK;
+}
+
+static int reset_histories(vdi_sim* S) {
+    cudaStream_t s = S->s;
+    size_t mn = size_t(S->prm.m) * S->prm.n, nf = size_t(S->prm.m + 1) * (S->prm.n + 1);
+    VDI_CUDA(cudaMemsetAsync(S->hist, 0, 4 * sizeof(GuessHist), s));
+    double* zs[] = {S->q, S->q_prev, S->zu, S->zu_prev, S->zv, S->zv_prev};
+    for (auto z : zs) VDI_CUDA(cudaMemsetAsync(z, 0, mn * sizeof(double), s));
+    VDI_CUDA(cudaMemsetAsync(S->zf, 0, nf * sizeof(double), s));
+    VDI_CUDA(cudaMemsetAsync(S->zf_prev, 0, nf * sizeof(double), s));
+    return VDI_OK;
+}
+
+int vdi_sim_init_fields(vdi_sim* S) {
+    if (!S) return VDI_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = S->s;
+    size_t NG = ghosted(S);
+    VDI_CUDA(cudaMemsetAsync(S->f.u, 0, NG * 8, s));
+    VDI_CUDA(cudaMemsetAsync(S->f.v, 0, NG * 8, s));
+    VDI_CUDA(cudaMemsetAsync(S->f.p, 0, NG * 8, s));
+    VDI_CUDA(cudaMemsetAsync(S->gas.tau, 0, (S->prm.m + 4) * 8, s));
+    double tv[2] = {0., S->prm.V};
+    VDI_CUDA(cudaMemcpyAsync(S->d_time, tv, sizeof(tv), cudaMemcpyHostToDevice, s));
+    VDI_TRY(reset_histories(S));
+    VDI_TRY(launch_gas_init(s, S->gp, S->gas, S->prm.h0, S->prm.V));
+    VDI_TRY(launch_inviscid_bc(s, S->g, S->f, S->gas, 0.));
+    VDI_TRY(launch_viscous_bc(s, S->g, S->f, S->gas));
+    VDI_CUDA(cudaStreamSynchronize(s));
+    return VDI_OK;
+}
+
+int vdi_sim_timestep_select(const vdi_sim* S, double interval, double* adt, int* nsteps) {
+    if (!S || !adt) return VDI_ERR_INVALID_ARGUMENT;
+    int l = static_cast<int>(interval / S->dt_reg) + 1;   // fluid_2d.hh:82-86
+    *adt = interval / l;
+    if (nsteps) *nsteps = l;
+    return VDI_OK;
+}
+
+int vdi_sim_step_forward(vdi_sim* S, double dt, int nsteps) {
+    if (!S || !(dt > 0) || nsteps < 0) return VDI_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < nsteps; k++) {
+        if (S->use_graph) {
+            if (!S->gexec || S->graph_dt != dt) VDI_TRY(capture_step(S, dt));
+            VDI_CUDA(cudaGraphLaunch(S->gexec, S->s));
+        } else {
+            VDI_TRY(update_visc(S, dt));
+            VDI_TRY(enqueue_step(S, dt));
+        }
+        S->steps++;
+    }
+    return check_errors(S);
+}
+
+int vdi_sim_use_graph(vdi_sim* S, int enable) {
+    if (!S) return VDI_ERR_INVALID_ARGUMENT;
+    S->use_graph = enable != 0;
+    if (!S->use_graph) destroy_graph(S);
+    return VDI_OK;
+}
+
+int vdi_sim_synchronize(vdi_sim* S) {
+    if (!S) return VDI_ERR_INVALID_ARGUMENT;
+    return check_errors(S);
+}
+
+int vdi_sim_get_state(vdi_sim* S, vdi_state* h) {
+    if (!S || !h) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    size_t NG = ghosted(S) * 8;
+    int m = S->prm.m;
+    struct {
+        double* dst;
+        const double* src;
+        size_t bytes;
+    } cp[] = {{h->u, S->f.u, NG},        {h->v, S->f.v, NG},          {h->p, S->f.p, NG},
+              {h->gp, S->gas.gp, (m + 1) * 8u}, {h->tau, S->gas.tau, (m + 4) * 8u}, {h->h, S->gas.h, m * 8u},
+              {h->fbd, S->gas.fbd, m * 8u}, {h->pg, S->gas.pg, (m + 1) * 8u}, {h->ht, S->gas.ht, m * 8u}};
+    for (auto& c : cp)
+        if (c.dst) VDI_CUDA(cudaMemcpy(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost));
+    double tv[2];
+    VDI_CUDA(cudaMemcpy(tv, S->d_time, sizeof(tv), cudaMemcpyDeviceToHost));
+    h->time = tv[0];
+    h->Vframe = tv[1];
+    return VDI_OK;
+}
+
+int vdi_sim_set_state(vdi_sim* S, const vdi_state* h) {
+    if (!S || !h || !h->u || !h->v || !h->p || !h->gp || !h->tau || !h->h || !h->fbd || !h->pg || !h->ht)
+        return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    size_t NG = ghosted(S) * 8;
+    int m = S->prm.m;
+    struct {
+        double* dst;
+        const double* src;
+        size_t bytes;
+    } cp[] = {{S->f.u, h->u, NG},        {S->f.v, h->v, NG},          {S->f.p, h->p, NG},
+              {S->gas.gp, h->gp, (m + 1) * 8u}, {S->gas.tau, h->tau, (m + 4) * 8u}, {S->gas.h, h->h, m * 8u},
+              {S->gas.fbd, h->fbd, m * 8u}, {S->gas.pg, h->pg, (m + 1) * 8u}, {S->gas.ht, h->ht, m * 8u}};
+    for (auto& c : cp) VDI_CUDA(cudaMemcpy(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice));
+    double tv[2] = {h->time, h->Vframe};
+    VDI_CUDA(cudaMemcpy(S->d_time, tv, sizeof(tv), cudaMemcpyHostToDevice));
+    // hx is derived from h, as the reference's restart loader does
+    // (gas_layer_solve.cc:318); the multigrid history restarts (mgs_common.cc:22-27)
+    std::vector<double> hh(h->h, h->h + m), hx(m + 1);
+    for (int i = 1; i < m; i++) hx[i] = S->gp.xsp * (hh[i] - hh[i - 1]);
+    hx[0] = S->prm.x_sym ? 0 : hx[1];
+    hx[m] = hx[m - 1];
+    VDI_CUDA(cudaMemcpy(S->gas.hx, hx.data(), (m + 1) * 8, cudaMemcpyHostToDevice));
+    VDI_TRY(reset_histories(S));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    return VDI_OK;
+}
+
+int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
+    if (!S || !out) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    memset(out, 0, sizeof(*out));
+    out->steps = S->steps;
+    for (int k = 0; k < 4; k++) {
+        if (!S->mg[k]) continue;
+        SolveCtl c;
+        VDI_CUDA(cudaMemcpy(&c, mg_ctl(S->mg[k]), sizeof(SolveCtl), cudaMemcpyDeviceToHost));
+        out->solves[k] = long(c.solves);
+        out->vcycles[k] = long(c.vcycles);
+        out->last_rel_res[k] = c.last_rel;
+        if (reset) {
+            c.solves = 0;
+            c.vcycles = 0;
+            VDI_CUDA(cudaMemcpy(mg_ctl(S->mg[k]), &c, sizeof(SolveCtl), cudaMemcpyHostToDevice));
+        }
+    }
+    GasStats gs;
+    VDI_CUDA(cudaMemcpy(&gs, S->d_gstats, sizeof(gs), cudaMemcpyDeviceToHost));
+    out->newton_steps = long(gs.newton_steps);
+    out->tri_pivot_fallbacks = long(gs.pivot_fallbacks);
+    out->height_fixed_point_iters = long(gs.fixed_point_iters);
+    if (reset) {
+        VDI_CUDA(cudaMemset(S->d_gstats, 0, sizeof(GasStats)));
+        S->steps = 0;
+    }
+    return VDI_OK;
+}
+
+int vdi_sim_device_field(vdi_sim* S, int which, double** d_ptr, size_t* count) {
+    if (!S || !d_ptr) return VDI_ERR_INVALID_ARGUMENT;
+    int m = S->prm.m;
+    switch (which) {
+        case 0: *d_ptr = S->f.u; if (count) *count = ghosted(S); break;
+        case 1: *d_ptr = S->f.v; if (count) *count = ghosted(S); break;
+        case 2: *d_ptr = S->f.p; if (count) *count = ghosted(S); break;
+        case 3: *d_ptr = S->gas.h; if (count) *count = m; break;
+        case 4: *d_ptr = S->gas.pg; if (count) *count = m + 1; break;
+        case 5: *d_ptr = S->gas.gp; if (count) *count = m + 1; break;
+        default: return VDI_ERR_INVALID_ARGUMENT;
+    }
+    return VDI_OK;
+}
+
+// ------------------------------------------------------------ multigrid
+struct vdi_mg {
+    MG* g = nullptr;
+    cudaStream_t s = nullptr;
+};
+
+int vdi_mg_create(int kind, int m, int n, double c1, double c2, int x_sym, void* stream, vdi_mg** out) {
+    if (!out) return VDI_ERR_INVALID_ARGUMENT;
+    vdi_mg* h = new vdi_mg();
+    h->s = static_cast<cudaStream_t>(stream);
+    double a = c1, b = c2;
+    if (kind == VDI_MG_MAC) {
+        // mgs_mac.cc:23-27 (test constructor): xxsp = 1/(dx*dx)
+        a = 1. / (c1 * c1);
+        b = 1. / (c2 * c2);
+    }
+    int st = mg_create(kind, m, n, a, b, x_sym, &h->g);
+    if (st != VDI_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return VDI_OK;
+}
+
+int vdi_mg_destroy(vdi_mg* h) {
+    if (!h) return VDI_OK;
+    if (h->g) mg_destroy(h->g);
+    delete h;
+    return VDI_OK;
+}
+
+int vdi_mg_setup(vdi_mg* h) { return h ? VDI_OK : VDI_ERR_INVALID_ARGUMENT; }
+
+int vdi_mg_solve(vdi_mg* h, const double* d_b, double* d_z, double rtol, int max_vcycles, int precision,
+                 vdi_mg_result* res) {
+    if (!h || !d_b || !d_z || !(rtol > 0) || max_vcycles < 0) return VDI_ERR_INVALID_ARGUMENT;
+    int v = 0;
+    double r = 0;
+    int st = mg_solve(h->g, h->s, d_b, d_z, rtol, max_vcycles, precision, &v, &r);
+    if (res) {
+        res->vcycles = v;
+        res->rel_res = r;
+    }
+    return st;
+}
+
+int vdi_mg_v_cycle(vdi_mg* h, const double* d_b, double* d_z) {
+    if (!h || !d_b || !d_z) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_TRY(mg_v_cycle(h->g, h->s, d_b, d_z));
+    VDI_CUDA(cudaStreamSynchronize(h->s));
+    return VDI_OK;
+}
+
+int vdi_mg_residual(vdi_mg* h, const double* d_b, const double* d_z, double* d_r, double* norm) {
+    if (!h || !d_b || !d_z) return VDI_ERR_INVALID_ARGUMENT;
+    return mg_residual(h->g, h->s, d_b, d_z, d_r, norm);
+}
+
+int vdi_mg_apply(vdi_mg* h, const double* d_z, double* d_y) {
+    if (!h || !d_z || !d_y) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_TRY(mg_apply(h->g, h->s, d_z, d_y));
+    VDI_CUDA(cudaStreamSynchronize(h->s));
+    return VDI_OK;
+}
+
+int vdi_tri_solve(int n, double* d_a, double* d_b, double* d_c, double* d_d, void* stream, int* pivoted) {
+    if (n < 2 || !d_a || !d_b || !d_c || !d_d) return VDI_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int* dp;
+    VDI_CUDA(cudaMallocAsync(&dp, sizeof(int), s));
+    VDI_TRY(launch_tri_solve(s, n, d_a, d_b, d_c, d_d, dp));
+    int hp = 0;
+    VDI_CUDA(cudaMemcpyAsync(&hp, dp, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VDI_CUDA(cudaFreeAsync(dp, s));
+    VDI_CUDA(cudaStreamSynchronize(s));
+    if (pivoted) *pivoted = hp > 0 ? 1 : 0;
+    if (hp < 0) {
+        set_error("tri_solve: zero pivot at row %d", -hp);
+        return VDI_ERR_TRI_SINGULAR;
+    }
+    return VDI_OK;
+}
+
+}  // extern "C"

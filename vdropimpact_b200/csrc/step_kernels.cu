@@ -1,0 +1,528 @@
+// Stencil kernels of one timestep of fluid_2d::step_forward
+// (fluid_2d.cc:93-405) and the boundary conditions of fluid_2d_sio.cc.
+//
+// Every field lives in its own FP64 array over the ghosted grid: (n+4) rows
+// of pitch P = m+4, cell (i,j) at (j+2)*P + i+2, i in [-2,m+1], j in [-2,n+1].
+// Expressions keep the reference's evaluation order; this file is compiled
+// with -fmad=false so that, given the same inputs, the results equal the
+// reference's double-precision results bit for bit.
+#include "step_kernels.hh"
+
+#include <cmath>
+
+namespace vdi {
+
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+// fluid_2d.cc:445-449
+__device__ __forceinline__ double delta_lim(double f0, double f1, double f2) {
+    double drm = f1 - f0, drp = f2 - f1;
+    return drm > 0 ? (drp > 0 ? 2 * dmin(drm, drp) : 0) : (drp > 0 ? 0 : -2 * dmax(drm, drp));
+}
+// fluid_2d.cc:434-437
+__device__ __forceinline__ double delta_f(double f0, double f1, double f2) {
+    double drc = 0.5 * (f2 - f0);
+    return drc > 0 ? dmin(drc, delta_lim(f0, f1, f2)) : dmax(drc, -delta_lim(f0, f1, f2));
+}
+// fluid_2d.cc:422-426
+__device__ __forceinline__ double mono_diff(double f0, double f1, double f2, double f3, double f4) {
+    double tdrc = f3 - f1, s = (1 / 6.) * (4 * tdrc - delta_f(f0, f1, f2) - delta_f(f2, f3, f4)),
+           t = delta_lim(f1, f2, f3);
+    return tdrc > 0 ? dmin(s, t) : dmax(s, -t);
+}
+// fluid_2d.cc:455-461
+__device__ __forceinline__ void godunov_set(double u0, double& u1, double v0, double& v1) {
+    if (u0 > -u1) {
+        if (u0 > 0) {
+            u1 = u0;
+            v1 = v0;
+            return;
+        }
+    } else if (u1 < 0)
+        return;
+    u1 = 0;
+    v1 = 0.5 * (v0 + v1);
+}
+// fluid_2d.cc:469-476
+__device__ __forceinline__ void godunov_set_tang(double& u0, double& u1, double v0, double& v1) {
+    if (u0 > -u1) {
+        if (u0 > 0) {
+            u1 = u0;
+            v1 = v0;
+            return;
+        }
+    } else if (u1 < 0) {
+        u0 = u1;
+        return;
+    }
+    v1 = 0.5 * (v0 + v1);
+    u0 = 0.5 * (u0 + u1);
+    u1 = 0;
+}
+
+#define CELL_LOOP                                                    \
+    int i = blockIdx.x * blockDim.x + threadIdx.x;                   \
+    int j = blockIdx.y * blockDim.y + threadIdx.y;                   \
+    if (i >= g.m || j >= g.n) return;                                \
+    const int P = g.m + 4;                                           \
+    const int c = (j + 2) * P + i + 2;
+
+// -------------------------------------------------------------- stage 1
+// fluid_2d.cc:105-132, then zero_edge_velocities (fluid_2d.cc:480-482)
+__global__ void k_stage1(Grid g, Fields f, double dt) {
+    CELL_LOOP
+    const double* u = f.u;
+    const double* v = f.v;
+    double uc = u[c], vc = v[c];
+    double uy = g.ysp * mono_diff(u[c - 2 * P], u[c - P], uc, u[c + P], u[c + 2 * P]);
+    double vy = g.ysp * mono_diff(v[c - 2 * P], v[c - P], vc, v[c + P], v[c + 2 * P]);
+    double ux = g.xsp * mono_diff(u[c - 2], u[c - 1], uc, u[c + 1], u[c + 2]);
+    double vx = g.xsp * mono_diff(v[c - 2], v[c - 1], vc, v[c + 1], v[c + 2]);
+    f.uy[c] = uy; f.vy[c] = vy; f.ux[c] = ux; f.vx[c] = vx;
+    f.ud[c] = uc - 0.5 * (g.dy + dt * vc) * uy;
+    f.vd[c] = vc - 0.5 * (g.dy + dt * vc) * vy;
+    f.ul[c] = (g.x_sym && i == 0) ? 0. : uc - 0.5 * (g.dx + dt * uc) * ux;
+    f.vl[c] = vc - 0.5 * (g.dx + dt * uc) * vx;
+    f.ur[c] = uc + 0.5 * (g.dx - dt * uc) * ux;
+    f.vr[c] = vc + 0.5 * (g.dx - dt * uc) * vx;
+    f.uu[c] = uc + 0.5 * (g.dy - dt * vc) * uy;
+    f.vu[c] = vc + 0.5 * (g.dy - dt * vc) * vy;
+}
+
+// -------------------------------------------------------------- stage 2
+// fluid_2d.cc:137-150. Each edge value is written by exactly one thread.
+__global__ void k_stage2(Grid g, Fields f) {
+    CELL_LOOP
+    if (i < g.m - 1) {
+        double u0 = f.ur[c], u1 = f.ul[c + 1], v1 = f.vl[c + 1];
+        godunov_set_tang(u0, u1, f.vr[c], v1);
+        f.ur[c] = u0; f.ul[c + 1] = u1; f.vl[c + 1] = v1;
+        if (i == 0) f.ur[c - 1] = f.ul[c];
+    } else {
+        f.ul[c + 1] = f.ur[c];
+        f.vl[c + 1] = f.vr[c];
+    }
+    if (j < g.n - 1) {
+        double u0 = f.vu[c], u1 = f.vd[c + P], v1 = f.ud[c + P];
+        godunov_set_tang(u0, u1, f.uu[c], v1);
+        f.vu[c] = u0; f.vd[c + P] = u1; f.ud[c + P] = v1;
+        if (j == 0) f.vu[c - P] = f.vd[c];
+    } else {
+        f.vd[c + P] = f.vu[c];
+        f.ud[c + P] = f.uu[c];
+    }
+}
+
+// ---------------------------------------------------------- stages 3-4
+// fluid_2d.cc:153-201: transverse terms, then half-step edge velocities and
+// the viscous force (written to the second edge set and fc0/fc1).
+__global__ void k_stage34(Grid g, Fields f, double dt) {
+    CELL_LOOP
+    double c0 = 0.5 * g.xsp * (f.ul[c + 1] + f.ul[c]) * (f.ur[c] - f.ur[c - 1]);
+    double c1 = 0.5 * g.xsp * (f.ul[c + 1] + f.ul[c]) * (f.vl[c + 1] - f.vl[c]);
+    double c2 = 0.5 * g.ysp * (f.vd[c + P] + f.vd[c]) * (f.ud[c + P] - f.ud[c]);
+    double c3 = 0.5 * g.ysp * (f.vd[c + P] + f.vd[c]) * (f.vu[c] - f.vu[c - P]);
+    const double* u = f.u;
+    const double* v = f.v;
+    const double* p = f.p;
+    double uc = u[c], vc = v[c];
+    double px = 0.5 * g.xsp * (p[c + P + 1] + p[c + 1] - p[c + P] - p[c]);
+    double py = 0.5 * g.ysp * (p[c + P + 1] - p[c + 1] + p[c + P] - p[c]);
+    // centered_diff, fluid_2d.cc:412-417
+    double uyy = g.yysp * (u[c - P] - 2 * uc + u[c + P]);
+    double vyy = g.yysp * (v[c - P] - 2 * vc + v[c + P]);
+    double uxx = g.xxsp * (u[c - 1] - 2 * uc + u[c + 1]);
+    double vxx = g.xxsp * (v[c - 1] - 2 * vc + v[c + 1]);
+    double f_x = -px * g.rhoinv + g.viscfac * (uxx + uyy);
+    double f_y = -py * g.rhoinv + g.viscfac * (vxx + vyy);
+    double ux = f.ux[c], uy = f.uy[c], vx = f.vx[c], vy = f.vy[c];
+    f.ud2[c] = uc + 0.5 * (-g.dy * uy + dt * (-c0 - vc * uy + f_x));
+    f.vd2[c] = vc + 0.5 * (-g.dy * vy + dt * (-c1 - vc * vy + f_y));
+    f.ul2[c] = uc + 0.5 * (-g.dx * ux + dt * (-uc * ux - c2 + f_x));
+    f.vl2[c] = vc + 0.5 * (-g.dx * vx + dt * (-uc * vx - c3 + f_y));
+    f.ur2[c] = uc + 0.5 * (g.dx * ux + dt * (-uc * ux - c2 + f_x));
+    f.vr2[c] = vc + 0.5 * (g.dx * vx + dt * (-uc * vx - c3 + f_y));
+    f.uu2[c] = uc + 0.5 * (g.dy * uy + dt * (-c0 - vc * uy + f_x));
+    f.vu2[c] = vc + 0.5 * (g.dy * vy + dt * (-c1 - vc * vy + f_y));
+    f.fc0[c] = g.viscfac * (uxx + uyy);
+    f.fc1[c] = g.viscfac * (vxx + vyy);
+}
+
+// ---------------------------------------------------------- stage 5 + 6
+// fluid_2d.cc:205-232: zero_edge_velocities, normal upwinding, and the MAC
+// source with the bottom Dirichlet term. Every thread recomputes the
+// upwinded values of its own four edges from the stage-4 set, writes the
+// left and bottom ones (and the ghost ones at the right and top), and forms
+// the divergence.
+__global__ void k_stage5_src(Grid g, Fields f, Gas gs, double dt, double* __restrict__ src) {
+    CELL_LOOP
+    // left edge of (i,j)
+    double ulL, vlL;
+    if (i == 0) {
+        ulL = g.x_sym ? 0. : f.ul2[c];
+        vlL = f.vl2[c];
+    } else {
+        ulL = f.ul2[c];
+        vlL = f.vl2[c];
+        godunov_set(f.ur2[c - 1], ulL, f.vr2[c - 1], vlL);
+    }
+    // right edge
+    double ulR, vlR;
+    if (i < g.m - 1) {
+        ulR = f.ul2[c + 1];
+        vlR = f.vl2[c + 1];
+        godunov_set(f.ur2[c], ulR, f.vr2[c], vlR);
+    } else {
+        ulR = f.ur2[c];
+        vlR = f.vr2[c];
+        f.ul[c + 1] = ulR;
+        f.vl[c + 1] = vlR;
+    }
+    // bottom edge
+    double vdB, udB;
+    if (j == 0) {
+        vdB = f.vd2[c];
+        udB = f.ud2[c];
+    } else {
+        vdB = f.vd2[c];
+        udB = f.ud2[c];
+        godunov_set(f.vu2[c - P], vdB, f.uu2[c - P], udB);
+    }
+    // top edge
+    double vdT, udT;
+    if (j < g.n - 1) {
+        vdT = f.vd2[c + P];
+        udT = f.ud2[c + P];
+        godunov_set(f.vu2[c], vdT, f.uu2[c], udT);
+    } else {
+        vdT = f.vu2[c];
+        udT = f.uu2[c];
+        f.vd[c + P] = vdT;
+        f.ud[c + P] = udT;
+    }
+    f.ul[c] = ulL; f.vl[c] = vlL; f.vd[c] = vdB; f.ud[c] = udB;
+    double s = g.xsp * (ulR - ulL) + g.ysp * (vdT - vdB);
+    if (j == 0) {
+        const double macfac = 0.125 * g.rhoinv * dt;
+        double sbc = macfac * (gs.gp_old[i] + gs.gp_old[i + 1] + gs.gp[i] + gs.gp[i + 1]);
+        s -= 2 * g.yysp * sbc;
+    }
+    src[i + g.m * j] = s;
+}
+
+// ------------------------------------------- MAC correction + advection
+// fluid_2d.cc:236-261, with the corrected edge velocities formed on the fly.
+// Also advances the simulation time by dt/2 (fluid_2d.cc:251).
+__global__ void k_mac_advect(Grid g, Fields f, Gas gs, const double* __restrict__ q, double dt, double* d_time) {
+    CELL_LOOP
+    const int m = g.m;
+    const int ij = i + m * j;
+    double ulL = f.ul[c];
+    if (i >= 1) ulL -= (q[ij] - q[ij - 1]) * g.xsp;
+    double ulR = f.ul[c + 1];
+    if (i + 1 <= m - 1) ulR -= (q[ij + 1] - q[ij]) * g.xsp;
+    double vdB = f.vd[c];
+    if (j >= 1) {
+        vdB -= (q[ij] - q[ij - m]) * g.ysp;
+    } else {
+        const double macfac = 0.125 * g.rhoinv * dt;
+        double sbc = macfac * (gs.gp_old[i] + gs.gp_old[i + 1] + gs.gp[i] + gs.gp[i + 1]);
+        vdB -= 2 * g.ysp * (q[ij] - sbc);
+    }
+    double vdT = f.vd[c + P];
+    if (j + 1 <= g.n - 1) vdT -= (q[ij + m] - q[ij]) * g.ysp;
+    double uc = f.u[c], vc = f.v[c];
+    f.fc0[c] = uc + dt * (-0.5 * (g.xsp * (ulR + ulL) * (ulR - ulL) + g.ysp * (vdT + vdB) * (f.ud[c + P] - f.ud[c])) +
+                          f.fc0[c]);
+    f.fc1[c] = vc + dt * (-0.5 * (g.xsp * (ulR + ulL) * (f.vl[c + 1] - f.vl[c]) + g.ysp * (vdT + vdB) * (vdT - vdB)) +
+                          f.fc1[c]);
+    if (i == 0 && j == 0) *d_time += 0.5 * dt;
+}
+
+// -------------------------------------------------- inviscid boundaries
+// fluid_2d_sio.cc:256-290 and 366-405: far-field ghost velocities stepped
+// with a composite Simpson integral of the base pressure. One warp per ghost
+// point; lanes split the quadrature nodes and reduce with shuffles.
+__global__ void k_inviscid_bc(Grid g, Fields f, Gas gs, double dt) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    const int m = g.m, n = g.n, ml = m + 4, P = m + 4, me = m + 1;
+    int total = 2 * n + 2 * ml;
+    if (warp >= total) return;
+    double x, y;
+    int idx;     // ghosted array index of the ghost cell
+    int right_row = -1;
+    if (warp < 2 * n) {
+        int j = warp >> 1, outer = warp & 1;
+        x = g.bx + g.dx * (outer ? 1.5 : 0.5);
+        y = g.ay + (j + 0.5) * g.dy;
+        idx = (j + 2) * P + m + 2 + outer;
+        right_row = j;
+    } else {
+        int k = warp - 2 * n;
+        int col = k >> 1, outer = k & 1;
+        x = g.ax + (col - 1.5) * g.dx;
+        y = g.by + g.dy * (outer ? 1.5 : 0.5);
+        idx = (n + 2 + outer) * P + col;
+    }
+    const double prefac = g.dx * g.rhoinv * dt / (3 * M_PI);
+    const double xm0 = x - g.ax, xp0 = x + g.ax, ysq = y * y;
+    double su = 0, sv = 0;
+    for (int jq = lane; jq < me; jq += 32) {
+        double xms = xm0 - jq * g.dx, xps = xp0 + jq * g.dx, pp = gs.gp[jq];
+        double rm = xms * xms + ysq;
+        rm = 1 / (rm * rm);
+        double fsu, fsv;
+        if (g.x_sym) {
+            double rp = xps * xps + ysq;
+            rp = 1 / (rp * rp);
+            fsu = pp * (xms * rm + xps * rp);
+            fsv = -pp * ((xms * xms - ysq) * rm + (xps * xps - ysq) * rp);
+        } else {
+            fsu = pp * xms * rm;
+            fsv = -pp * (xms * xms - ysq) * rm;
+        }
+        double w = (jq == 0 || jq == me - 1) ? 1. : ((jq & 1) ? 4. : 2.);
+        su += w * fsu;
+        sv += w * fsv;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        su += __shfl_down_sync(0xffffffffu, su, o);
+        sv += __shfl_down_sync(0xffffffffu, sv, o);
+    }
+    if (lane == 0) {
+        double un = f.u[idx] + 2 * y * prefac * su;
+        double vn = f.v[idx] + prefac * sv;
+        f.u[idx] = un;
+        f.v[idx] = vn;
+        if (right_row >= 0 && !g.x_sym) {
+            // fluid_2d_sio.cc:271-276: mirror onto the left ghosts
+            int j = right_row, outer = warp & 1;
+            int li = (j + 2) * P + (outer ? 0 : 1);
+            f.u[li] = -un;
+            f.v[li] = vn;
+        }
+    }
+}
+
+// --------------------------------------------------- viscous boundaries
+// fluid_2d_sio.cc:294-343 in one CTA (three dependent phases).
+__global__ void k_viscous_bc(Grid g, Fields f, Gas gs) {
+    const int m = g.m, n = g.n, P = m + 4, ml = m + 4;
+    double* u = f.u;
+    double* v = f.v;
+    if (g.x_sym) {
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            int c = (j + 2) * P + 2;
+            u[c - 1] = -u[c];
+            v[c - 1] = v[c];
+            u[c - 2] = -u[c + 1];
+            v[c - 2] = v[c + 1];
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < ml; k += blockDim.x) {
+        double un_edge = g.muinv * gs.tau[k];
+        u[P + k] = u[2 * P + k] - g.dy * un_edge;
+        u[k] = u[3 * P + k] - 3 * g.dy * un_edge;
+    }
+    __syncthreads();
+    for (int k = 1 + threadIdx.x; k < m + 2; k += blockDim.x) {
+        double uxa = 0.5 * g.xsp * (u[P + k + 1] - u[P + k - 1]);
+        double uxb = 0.5 * g.xsp * (u[k + 1] - u[k - 1]);
+        double v1 = v[2 * P + k] + g.dy * uxa;
+        v[P + k] = v1;
+        v[k] = v1 + g.dy * uxb;
+    }
+}
+
+// ------------------------------------------------------- viscous sources
+// fluid_2d.cc:279-324: right-hand sides of the u and v systems.
+__global__ void k_visc_rhs(Grid g, Fields f, Gas gs, double vfx, double vfy, double* __restrict__ su,
+                           double* __restrict__ sv) {
+    CELL_LOOP
+    const double* u = f.u;
+    const double* v = f.v;
+    double a = f.fc0[c], b = f.fc1[c];
+    if (!g.x_sym && i == 0) {
+        a += vfx * u[c - 1];
+        b += vfx * v[c - 1];
+    }
+    if (i == g.m - 1) {
+        a += vfx * u[c + 1];
+        b += vfx * v[c + 1];
+    }
+    if (j == g.n - 1) {
+        a += vfy * u[c + P];
+        b += vfy * v[c + P];
+    }
+    if (j == 0) {
+        double dudy = g.muinv * 0.5 * (gs.tau_old[i + 2] + gs.tau[i + 2]);
+        a -= vfy * g.dy * dudy;
+        double dvdy = -0.5 * g.xsp * (u[c + 1] - u[c - 1]);
+        b -= vfy * g.dy * dvdy;
+    }
+    su[i + g.m * j] = a;
+    sv[i + g.m * j] = b;
+}
+
+// ------------------------------------------------------------ FEM source
+// fluid_2d.cc:337-377 on the (m+1) x (n+1) nodes; vel0/vel1 are the
+// provisional velocities (the viscous solutions when implicit).
+__global__ void k_fem_rhs(Grid g, Fields f, Gas gs, CellView c0v, CellView c1v, double dt, double a_cc_edge,
+                          double a_cc_mid, double* __restrict__ src) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int m = g.m, n = g.n, me = m + 1, P = m + 4;
+    if (i > m || j > n) return;
+    if (j == 0) {
+        // fluid_2d.cc:377 with mgs_fem::a_cc(i,i) (mgs_fem.hh:55-57)
+        src[i] = ((i > 0 && i < m) ? a_cc_mid : a_cc_edge) * gs.gp[i];
+        return;
+    }
+    double spx = 0, spy = 0;
+    if (i != 0) {
+        spx += c0v.at(i - 1, j - 1);
+        spy += c1v.at(i - 1, j - 1);
+    }
+    if (i != 0 && j < n) {
+        spx += c0v.at(i - 1, j);
+        spy -= c1v.at(i - 1, j);
+    }
+    if (i != m) {
+        spx -= c0v.at(i, j - 1);
+        spy += c1v.at(i, j - 1);
+    }
+    if (i != m && j < n) {
+        spx -= c0v.at(i, j);
+        spy -= c1v.at(i, j);
+    }
+    double s = 0.5 * (g.dy * spx + g.dx * spy) * g.rho / dt;
+    const double* u = f.u;
+    const double* v = f.v;
+    const double fl = 0.25 * g.dy * g.rho / dt;
+    if (!g.x_sym && i == 0) {
+        if (j < n) s += fl * (c0v.at(0, j) + u[(j + 2) * P + 1]);
+        s += fl * (c0v.at(0, j - 1) + u[(j + 1) * P + 1]);
+    }
+    if (i == m) {
+        if (j < n) s -= fl * (c0v.at(m - 1, j) + u[(j + 2) * P + m + 2]);
+        s -= fl * (c0v.at(m - 1, j - 1) + u[(j + 1) * P + m + 2]);
+    }
+    if (j == n) {
+        const double ft = 0.25 * g.dx * g.rho / dt;
+        if (i > 0) s -= ft * (c1v.at(i - 1, n - 1) + v[(n + 2) * P + i + 1]);
+        if (i < m) s -= ft * (c1v.at(i, n - 1) + v[(n + 2) * P + i + 2]);
+    }
+    src[i + me * j] = s;
+}
+
+// ------------------------------------------------------ velocity update
+// fluid_2d.cc:383-396.
+__global__ void k_vel_update(Grid g, Fields f, CellView c0v, CellView c1v, const double* __restrict__ z, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int m = g.m, n = g.n, me = m + 1, P = m + 4;
+    if (i > m || j > n) return;
+    int c = (j + 2) * P + i + 2;
+    const double* sop = z + i + me * j;
+    f.p[c] = *sop;
+    if (i < m && j < n) {
+        f.u[c] = c0v.at(i, j) - 0.5 * dt * g.rhoinv * g.xsp * (sop[me + 1] + sop[1] - sop[me] - *sop);
+        f.v[c] = c1v.at(i, j) - 0.5 * dt * g.rhoinv * g.ysp * (sop[me + 1] - sop[1] + sop[me] - *sop);
+    }
+}
+
+// ------------------------------------------------ multigrid initial guess
+// mgs_common::initial_guess (mgs_common.cc:17-50). The decision is made from
+// device-resident times so that a captured graph replays it correctly.
+__global__ void k_guess_apply(double* __restrict__ z, double* __restrict__ zprev, int n, const GuessHist* h,
+                              const double* d_time) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int sc = h->scount;
+    if (sc < 2) {
+        if (sc == 1) zprev[k] = z[k];
+        return;
+    }
+    double t = *d_time;
+    if (fabs(h->t0 - h->t_prev) < 2.220446049250313e-16 * 10) return;
+    double a = 1. / (h->t0 - h->t_prev), b = (t - h->t_prev) * a, cc = (t - h->t0) * a;
+    double zz = z[k];
+    z[k] = b * zz - cc * zprev[k];
+    zprev[k] = zz;
+}
+
+__global__ void k_guess_finish(GuessHist* h, const double* d_time, int* err) {
+    double t = *d_time;
+    if (h->scount < 2) {
+        if (h->scount == 1) h->t0 = t;
+        else h->t_prev = t;
+        h->scount++;
+    } else {
+        if (fabs(h->t0 - h->t_prev) < 2.220446049250313e-16 * 10) {
+            atomicOr(err, DEV_DUP_TIME);
+            return;
+        }
+        h->t_prev = h->t0;
+        h->t0 = t;
+    }
+}
+
+// --------------------------------------------------------------- launch
+static dim3 cell_grid(int m, int n) { return dim3((m + 31) / 32, (n + 7) / 8); }
+static const dim3 CELL_BLOCK(32, 8);
+
+int launch_stage1(cudaStream_t s, const Grid& g, const Fields& f, double dt) {
+    k_stage1<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, dt);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_stage2(cudaStream_t s, const Grid& g, const Fields& f) {
+    k_stage2<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_stage34(cudaStream_t s, const Grid& g, const Fields& f, double dt) {
+    k_stage34<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, dt);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_stage5_src(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double dt, double* src) {
+    k_stage5_src<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, gs, dt, src);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_mac_advect(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, const double* q, double dt,
+                      double* d_time) {
+    k_mac_advect<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, gs, q, dt, d_time);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_inviscid_bc(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double dt) {
+    long warps = 2L * g.n + 2L * (g.m + 4);
+    k_inviscid_bc<<<int((warps * 32 + 255) / 256), 256, 0, s>>>(g, f, gs, dt);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_viscous_bc(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs) {
+    k_viscous_bc<<<1, 1024, 0, s>>>(g, f, gs);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_visc_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double vfx, double vfy,
+                    double* su, double* sv) {
+    k_visc_rhs<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, gs, vfx, vfy, su, sv);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_fem_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, CellView c0, CellView c1, double dt,
+                   double a_cc_edge, double a_cc_mid, double* src) {
+    k_fem_rhs<<<cell_grid(g.m + 1, g.n + 1), CELL_BLOCK, 0, s>>>(g, f, gs, c0, c1, dt, a_cc_edge, a_cc_mid, src);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c0, CellView c1, const double* z,
+                      double dt) {
+    k_vel_update<<<cell_grid(g.m + 1, g.n + 1), CELL_BLOCK, 0, s>>>(g, f, c0, c1, z, dt);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_guess(cudaStream_t s, double* z, double* zprev, int n, GuessHist* h, const double* d_time, int* err) {
+    k_guess_apply<<<(n + 255) / 256, 256, 0, s>>>(z, zprev, n, h, d_time);
+    k_guess_finish<<<1, 1, 0, s>>>(h, d_time, err);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+
+}  // namespace vdi
