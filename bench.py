@@ -1,0 +1,326 @@
+"""Benchmark: Navier-Stokes timesteps per second of vdropimpact's per-step
+fluid solve on the 2048x1024 liquid-deposition workload (100 cSt drop,
+2048-cell gas layer), every linear solve to ||b-Az||/||b|| <= 1e-10.
+
+One step = fluid_2d::step_forward: gas-layer Newton/tridiagonal update,
+Godunov advection, MAC multigrid projection, two implicit viscous multigrid
+solves, FEM multigrid projection. Two solver configurations run back to
+back on the same workload:
+  plain  - FP64 V-cycles, time-extrapolated initial guess (the reference's
+           method on the GPU)
+  fast   - FP32 V-cycles inside FP64 iterative refinement (the headline)
+`value` is the headline configuration's steps/s, summed over ranks (each
+rank runs an independent replica of the simulation).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+CFG = os.path.join(ROOT, "tests", "golden", "ld_vis100.cfg")
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "vdi_ref_driver")
+METRIC = "NS steps/s @2048x1024, learned+mixed MG vs plain FP64 MG, same 1e-10 residual"
+WORKLOAD = "ld_vis100 drop impact, 2048x1024 liquid grid, 2048-cell gas layer"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", default="2048x1024")
+    ap.add_argument("--rtol", type=float, default=1e-10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", default="", help="run only 'plain' or 'fast' (profiling)")
+    ap.add_argument("--eager", action="store_true", help="launch kernels without CUDA graphs (profiling)")
+    return ap.parse_args()
+
+
+def cfg_text(grid: str) -> str:
+    m, n = grid.split("x")
+    lines = [l for l in open(CFG).read().splitlines() if not l.startswith("grid_points")]
+    return "\n".join(lines + [f"grid_points {m} {n}"]) + "\n"
+
+
+# ------------------------------------------------------------------ dist
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while the
+    timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- reference
+def cpu_reference(text: str, steps: int, warmup: int, threads: int | None = None) -> dict:
+    """The reference's OpenMP CPU path (built from its sources by
+    oracle/Makefile) timed on this host's cores."""
+    import tempfile
+    if not os.path.exists(REF_DRIVER):
+        return {"unavailable": "oracle/_ref/vdi_ref_driver not built (make -C oracle)"}
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "bench.cfg")
+        open(path, "w").write(text)
+        env = dict(os.environ)
+        nthreads = threads or os.cpu_count()
+        env["OMP_NUM_THREADS"] = str(nthreads)
+        env["VDI_MG_RTOL"] = "1e-10"
+        r = subprocess.run([REF_DRIVER, "time", path, str(steps), str(warmup)], capture_output=True, text=True,
+                           env=env, timeout=1800)
+        if r.returncode != 0:
+            return {"unavailable": f"reference driver failed: {r.stderr.strip()[:200]}"}
+        out = json.loads(r.stdout.strip().splitlines()[-1])
+        out["cores"] = nthreads
+        return out
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    text = cfg_text(args.grid)
+    # each "step" of this arm is one reference timestep; the run times
+    # args.steps of them after args.warmup untimed ones, capped so the whole
+    # run stays within a few minutes
+    steps = max(1, min(args.steps, 20))
+    warm = max(1, min(args.warmup, 3))
+    r = cpu_reference(text, steps, warm)
+    if "unavailable" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+        return
+    v = r["steps_per_s"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": ws,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": args.grid, "solver": "reference OpenMP path + TGMG-API CPU multigrid",
+                   "mg_rtol": 1e-10},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": r["cores"], "kind": "reference",
+                         "sample": f"{steps} timesteps after {warm} warm-up steps at {args.grid}"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "vcycles_per_solve": r["vcycles"] / max(r["solves"], 1),
+    }
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------- ours
+def time_config(V, torch, text, args, precision, stream, ws, clocks=None):
+    f = V.Fluid2D(text, mg_rtol=args.rtol, mg_precision=precision, graph=not args.eager, stream=stream)
+    f.init_fields()
+    dt = f.frame_dt()
+    f.step_forward(dt, args.warmup)
+    f.stats(reset=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if clocks:
+        clocks.start()
+    e0.record(stream)
+    f.step_forward(dt, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ck = clocks.stop() if clocks else None
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ms = dist_max(ms, ws)
+    st = f.stats()
+    solves = sum(st["solves"].values())
+    vc = {k: st["vcycles"][k] / max(st["solves"][k], 1) for k in st["vcycles"]}
+    return f, dt, ms, vc, st, ck, solves
+
+
+def e2e_run(V, torch, f, dt, stream, steps, ws):
+    """The same metric through the public API: each step is one
+    Fluid2D.step_forward call (C-ABI vdi_sim_step_forward with the host
+    timestep, which returns the step's device-side status), followed by a
+    device-to-host read of the step's result, the gas-layer height h(x) and
+    gas pressure, into pinned memory."""
+    dh, nh = f.device_field(3)
+    dp, npg = f.device_field(4)
+    hbuf = torch.empty(nh, dtype=torch.float64, pin_memory=True)
+    pbuf = torch.empty(npg, dtype=torch.float64, pin_memory=True)
+    hdev, pdev = _wrap(torch, dh, nh), _wrap(torch, dp, npg)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        f.step_forward(dt, 1)
+        with torch.cuda.stream(stream):
+            hbuf.copy_(hdev, non_blocking=True)
+            pbuf.copy_(pdev, non_blocking=True)
+        stream.synchronize()
+    e1.record(stream)
+    e1.synchronize()
+    ms = dist_max(e0.elapsed_time(e1), ws)
+    return ms, 8, 8 * (nh + npg)
+
+
+def _wrap(torch, ptr, n):
+    """A float64 CUDA tensor viewing n doubles at device address ptr."""
+    class _Iface:
+        def __init__(self):
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+                                             "version": 3, "strides": None}
+    return torch.as_tensor(_Iface(), device="cuda")
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+    torch.cuda.set_device(local)
+    sys.path.insert(0, ROOT)
+    import vdropimpact_b200 as V
+    text = cfg_text(args.grid)
+    stream = torch.cuda.Stream()
+    results = {}
+    modes = [("plain", "fp64"), ("fast", "mixed")]
+    if args.only:
+        modes = [m for m in modes if m[0] == args.only]
+    keep = None
+    for name, prec in modes:
+        clocks = ClockSampler(local) if name == "fast" or args.only else None
+        f, dt, ms, vc, st, ck, solves = time_config(V, torch, text, args, prec, stream, ws, clocks)
+        results[name] = dict(ms=ms, vc=vc, clocks=ck, solves=solves, newton=st["newton_steps"])
+        if name == modes[-1][0]:
+            keep = (f, dt)
+        else:
+            f.close()
+    head = results[modes[-1][0]]
+    ms_step = head["ms"] / args.steps
+    value = ws * 1e3 / ms_step
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": args.grid, "mg_rtol": args.rtol,
+                   "solver": "FP32 V-cycles in FP64 refinement, time-extrapolated guess, CUDA-graph step",
+                   "l2": "per-step working set (~0.9 GB) exceeds the 126 MB L2",
+                   "parallelism": f"replicas x{ws}"},
+        "clocks": head["clocks"],
+        "vcycles_per_solve": head["vc"],
+        "gpu_launches": None,
+    }
+    if "plain" in results:
+        p = results["plain"]
+        line["plain_fp64"] = {"steps_per_s": ws * 1e3 * args.steps / p["ms"], "ms_per_step": p["ms"] / args.steps,
+                              "vcycles_per_solve": p["vc"]}
+        line["speedup_vs_plain_fp64"] = p["ms"] / head["ms"]
+    f, dt = keep
+    if not args.no_e2e:
+        e2e_steps = max(3, min(args.steps, 50))
+        ms, bi, bo = e2e_run(V, torch, f, dt, stream, e2e_steps, ws)
+        line["e2e"] = {"value": ws * 1e3 * e2e_steps / ms, "unit": "steps/s", "h2d_bytes_per_step": bi,
+                       "d2h_bytes_per_step": bo}
+    f.close()
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        r = cpu_reference(text, 8, 2)
+        if "unavailable" not in r:
+            line["cpu_baseline"] = {"value": r["steps_per_s"], "unit": "steps/s", "cores": r["cores"],
+                                    "kind": "reference",
+                                    "sample": f"8 timesteps of the same workload after 2 warm-up steps"}
+        else:
+            line["cpu_baseline"] = {"value": None, "unavailable": r["unavailable"]}
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -13,7 +13,8 @@
 //                                       state file <in>; writes the state
 //   dump  <cfg> <nsteps> <every> <out>  like step, appending a state every
 //                                       <every> steps
-//   time  <cfg> <nsteps>                time nsteps; prints one JSON line
+//   time  <cfg> <nsteps> [<warmup>]     time nsteps after warmup untimed steps;
+//                                       prints one JSON line
 //   mac|fem <m> <n> <dx> <dy> <b> <z>   one solve with the test constructor
 //                                       (mgs_mac.cc:23-27, mgs_fem.cc:26-30)
 //                                       as mg_test.cc:20-35 does
@@ -127,6 +128,7 @@ static int run_steps(int argc,char** argv,bool dump,bool timed) {
     if(in) load_state(f,in);
     else f.init_fields();
     double dt=frame_dt(f);
+    if(timed&&argc>4) for(int k=atoi(argv[4]);k>0;k--) f.step_forward(dt);
     FILE* o=NULL;
     if(dump) {o=fopen(out,"wb");save_state(f,o);}
     tgmg_stats_t& st=tgmg_stats();
