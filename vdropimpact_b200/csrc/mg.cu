@@ -15,11 +15,15 @@
 // 9-point stencil. The bottom (liquid-gas) row is a Dirichlet row on every
 // level.
 //
-// Levels with many points run as one launch per operation over the whole
-// grid; once the remaining levels fit in shared memory, a single CTA runs the
-// rest of the V-cycle there. Solves end when ||b-Az||_2 <= rtol*||b||_2.
-// FP32 V-cycles inside FP64 iterative refinement reuse the same kernels with
-// T = float.
+// Each level of a V-cycle above the shared-memory threshold is two launches:
+//   PRE : nu1 Gauss-Seidel sweeps, residual, restriction to the coarse source
+//   POST: prolongation of the coarse correction, nu2 sweeps, and on the finest
+//         level the residual norm and the convergence decision
+// Both work on a shared-memory tile whose halo shrinks by one ring per colour
+// phase, so a tile computes exactly the values the neighbouring tiles compute
+// for the same points. The remaining coarse levels run in one CTA, entirely in
+// shared memory. Solves end when ||b-Az||_2 <= rtol*||b||_2. FP32 V-cycles
+// inside FP64 iterative refinement use the same kernels with T = float.
 #include "vdi_internal.hh"
 
 #include <algorithm>
@@ -31,6 +35,7 @@ namespace vdi {
 static constexpr int MAXLEV = 16;
 static constexpr int CTA_THREADS = 1024;
 static constexpr size_t CTA_SMEM_LIMIT = 200 * 1024;
+static constexpr int MAX_PARTIALS = 8192;
 
 // ------------------------------------------------------------------ reduce
 __device__ __forceinline__ double warp_sum(double v) {
@@ -59,18 +64,19 @@ __device__ double block_sum(double v) {
  * total summed over the partials in index order (deterministic). */
 __device__ bool grid_sum(double blocksum, Reduce rd, double* total) {
     __shared__ int last;
+    const int nb = gridDim.x * gridDim.y;
+    const int bid = blockIdx.x + gridDim.x * blockIdx.y;
     if (threadIdx.x == 0) {
-        rd.partials[blockIdx.x] = blocksum;
+        rd.partials[bid] = blocksum;
         __threadfence();
         unsigned t = atomicAdd(rd.counter, 1u);
-        last = (t == gridDim.x - 1);
+        last = (t == unsigned(nb - 1));
     }
     __syncthreads();
     if (!last) return false;
     __threadfence();
     double s = 0;
-    for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x)
-        s += __ldcg(rd.partials + k);
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) s += __ldcg(rd.partials + k);
     s = block_sum(s);
     if (threadIdx.x == 0) {
         *total = s;
@@ -121,7 +127,7 @@ __device__ void solve_decide(SolveCtl* ctl, double r2, int count_cycle, int use_
     if (use_cond) cudaGraphSetConditional(h, cont);
 }
 
-// ------------------------------------------------------- cell-centred ops
+// ------------------------------------------------------- operators
 template <typename T>
 struct CCc {
     int m, n;
@@ -131,34 +137,68 @@ struct CCc {
     signed char gL, gR, gD, gU;
 };
 
+template <typename T>
+struct FEMc {
+    int M, N;
+    T fm, fey, hey, fex, hex, fc;
+    T d[3][3], invd[3][3];
+};
+
 __device__ __forceinline__ int cls(int i, int m) { return i == 0 ? 0 : (i == m - 1 ? 2 : 1); }
 
-/** A z at (i,j) for a grid array with pitch m (neighbours outside the grid
- * do not contribute, as in mul_a of mgs_mac.hh:39-45 / visco_impl.hh:40-46). */
+/** Off-diagonal part of A z at (i,j); w points at z(i,j) in an array of
+ * row pitch P. Neighbours outside the grid do not contribute, as in mul_a
+ * of mgs_mac.hh:39-45 and visco_impl.hh:40-46. */
 template <typename T>
-__device__ __forceinline__ T cc_off(const CCc<T>& c, const T* z, int i, int j) {
-    int ij = i + c.m * j;
-    T xs = (i > 0 ? z[ij - 1] : T(0)) + (i < c.m - 1 ? z[ij + 1] : T(0));
-    T ys = (j > 0 ? z[ij - c.m] : T(0)) + (j < c.n - 1 ? z[ij + c.m] : T(0));
+__device__ __forceinline__ T cc_off(const CCc<T>& c, const T* w, int P, int i, int j) {
+    T xs = (i > 0 ? w[-1] : T(0)) + (i < c.m - 1 ? w[1] : T(0));
+    T ys = (j > 0 ? w[-P] : T(0)) + (j < c.n - 1 ? w[P] : T(0));
     return c.ox * xs + c.oy * ys;
 }
 
+/** mul_a of mgs_fem.cc:32-53 at (i,j); w points at z(i,j), row pitch P. */
 template <typename T>
-__device__ __forceinline__ T cc_resid(const CCc<T>& c, const T* z, const T* b, int i, int j) {
-    int ij = i + c.m * j;
-    return b[ij] - c.d[cls(i, c.m)][cls(j, c.n)] * z[ij] - cc_off(c, z, i, j);
+__device__ __forceinline__ T fem_off(const FEMc<T>& c, const T* w, int P, int i, int j) {
+    if (j == 0) return T(0);
+    const T* wm = w - P;
+    const int M = c.M;
+    if (j == c.N - 1) {
+        if (i == 0) return c.fc * wm[1] + c.hey * (*wm) + c.hex * w[1];
+        if (i == M - 1) return c.fc * wm[-1] + c.hey * (*wm) + c.hex * w[-1];
+        return c.fc * (wm[-1] + wm[1]) + c.fey * (*wm) + c.hex * (w[-1] + w[1]);
+    }
+    if (i == 0) return c.fc * (wm[1] + w[P + 1]) + c.hey * (*wm + w[P]) + c.fex * w[1];
+    if (i == M - 1) return c.fc * (wm[-1] + w[P - 1]) + c.hey * (*wm + w[P]) + c.fex * w[-1];
+    return c.fc * (wm[-1] + wm[1] + w[P - 1] + w[P + 1]) + c.fey * (*wm + w[P]) + c.fex * (w[-1] + w[1]);
 }
 
 template <typename T>
-__device__ __forceinline__ void cc_relax(const CCc<T>& c, T* z, const T* b, int i, int j) {
-    int ij = i + c.m * j;
-    z[ij] = (b[ij] - cc_off(c, z, i, j)) * c.invd[cls(i, c.m)][cls(j, c.n)];
+__device__ __forceinline__ T op_off(const CCc<T>& c, const T* w, int P, int i, int j) { return cc_off(c, w, P, i, j); }
+template <typename T>
+__device__ __forceinline__ T op_off(const FEMc<T>& c, const T* w, int P, int i, int j) { return fem_off(c, w, P, i, j); }
+template <typename T>
+__device__ __forceinline__ int op_m(const CCc<T>& c) { return c.m; }
+template <typename T>
+__device__ __forceinline__ int op_n(const CCc<T>& c) { return c.n; }
+template <typename T>
+__device__ __forceinline__ int op_m(const FEMc<T>& c) { return c.M; }
+template <typename T>
+__device__ __forceinline__ int op_n(const FEMc<T>& c) { return c.N; }
+
+template <class OP, typename T>
+__device__ __forceinline__ T op_resid(const OP& c, const T* w, T bv, int P, int i, int j) {
+    return bv - c.d[cls(i, op_m(c))][cls(j, op_n(c))] * (*w) - op_off(c, w, P, i, j);
+}
+template <class OP, typename T>
+__device__ __forceinline__ T op_relaxed(const OP& c, const T* w, T bv, int P, int i, int j) {
+    return (bv - op_off(c, w, P, i, j)) * c.invd[cls(i, op_m(c))][cls(j, op_n(c))];
 }
 
 /** Bilinear cell-centred prolongation of the coarse correction to fine cell
  * (i,j); ghost values are g * (boundary value) on each side. */
 template <typename T>
-__device__ __forceinline__ T cc_interp(const CCc<T>& f, const T* zc, int mc, int nc, int i, int j) {
+__device__ __forceinline__ T cc_interp(const CCc<T>& f, const T* zc, int i, int j) {
+    const int mc = f.m >> 1, nc = f.n >> 1;
     int I = i >> 1, J = j >> 1;
     int sx = (i & 1) ? 1 : -1, sy = (j & 1) ? 1 : -1;
     int Ix = I + sx, Jy = J + sy;
@@ -175,91 +215,237 @@ __device__ __forceinline__ T cc_interp(const CCc<T>& f, const T* zc, int mc, int
     return T(0.5625) * c00 + T(0.1875) * (c10 + c01) + T(0.0625) * c11;
 }
 
+/** Bilinear prolongation of node-centred corrections to fine node (i,j). */
 template <typename T>
-__global__ void cc_rb_sweep(CCc<T> c, T* __restrict__ z, const T* __restrict__ b, int color) {
-    int half = c.m >> 1;
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= half * c.n) return;
-    int j = k / half;
-    int i = 2 * (k - j * half) + ((j + color) & 1);
-    cc_relax(c, z, b, i, j);
+__device__ __forceinline__ T fem_interp(const FEMc<T>& f, const T* zc, int i, int j) {
+    if (j == 0) return T(0);
+    const int Mc = (f.M - 1) / 2 + 1;
+    int I = i >> 1, J = j >> 1;
+    bool ox = i & 1, oy = j & 1;
+    T c00 = zc[I + Mc * J];
+    if (!ox && !oy) return c00;
+    if (ox && !oy) return T(0.5) * (c00 + zc[I + 1 + Mc * J]);
+    if (!ox && oy) return T(0.5) * (c00 + zc[I + Mc * (J + 1)]);
+    return T(0.25) * (c00 + zc[I + 1 + Mc * J] + zc[I + Mc * (J + 1)] + zc[I + 1 + Mc * (J + 1)]);
 }
-
 template <typename T>
-__global__ void cc_resid_restrict(CCc<T> c, const T* __restrict__ z, const T* __restrict__ b,
-                                  T* __restrict__ bc) {
-    int mc = c.m >> 1, nc = c.n >> 1;
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= mc * nc) return;
-    int J = k / mc, I = k - J * mc;
-    int i = 2 * I, j = 2 * J;
-    T s = cc_resid(c, z, b, i, j) + cc_resid(c, z, b, i + 1, j) + cc_resid(c, z, b, i, j + 1) +
-          cc_resid(c, z, b, i + 1, j + 1);
-    bc[k] = T(0.25) * s;
-}
-
+__device__ __forceinline__ T op_interp(const CCc<T>& c, const T* zc, int i, int j) { return cc_interp(c, zc, i, j); }
 template <typename T>
-__global__ void cc_prolong_add(CCc<T> f, T* __restrict__ z, const T* __restrict__ zc) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= f.m * f.n) return;
-    int j = k / f.m, i = k - j * f.m;
-    z[k] += cc_interp(f, zc, f.m >> 1, f.n >> 1, i, j);
-}
+__device__ __forceinline__ T op_interp(const FEMc<T>& c, const T* zc, int i, int j) { return fem_interp(c, zc, i, j); }
 
-/** ||b - A z||^2 (accumulated in FP64) followed by the solve decision. */
+/** P^T r at coarse node (I,J) from a residual array with origin (ox,oy) and
+ * pitch P; zero on the Dirichlet bottom row. */
 template <typename T>
-__global__ void cc_resid_norm(CCc<T> c, const T* __restrict__ z, const T* __restrict__ b, Reduce rd,
-                              SolveCtl* ctl, int count_cycle, int use_cond,
-                              cudaGraphConditionalHandle h) {
-    double s = 0;
-    int tot = c.m * c.n;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
-        int j = k / c.m, i = k - j * c.m;
-        double r = double(cc_resid(c, z, b, i, j));
-        s += r * r;
+__device__ __forceinline__ T fem_restrict_at(int M, int N, const T* r, int P, int ox, int oy, int I, int J) {
+    if (J == 0) return T(0);
+    T s = 0;
+    for (int dj = -1; dj <= 1; dj++) {
+        int j = 2 * J + dj;
+        if (j < 0 || j >= N) continue;
+        T wy = dj == 0 ? T(1) : T(0.5);
+        for (int di = -1; di <= 1; di++) {
+            int i = 2 * I + di;
+            if (i < 0 || i >= M) continue;
+            T wx = di == 0 ? T(1) : T(0.5);
+            s += wx * wy * r[(i - ox) + P * (j - oy)];
+        }
     }
-    s = block_sum(s);
-    double total;
-    if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
+    return s;
 }
 
-/** FP64 residual of an FP64 iterate written as FP32 (the refinement step),
- * with its FP64 norm and the solve decision. */
-__global__ void cc_resid_to32(CCc<double> c, const double* __restrict__ z, const double* __restrict__ b,
-                              float* __restrict__ r32, Reduce rd, SolveCtl* ctl, int count_cycle,
-                              int use_cond, cudaGraphConditionalHandle h) {
-    double s = 0;
-    int tot = c.m * c.n;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
-        int j = k / c.m, i = k - j * c.m;
-        double r = cc_resid(c, z, b, i, j);
-        r32[k] = float(r);
-        s += r * r;
+// ------------------------------------------------------- fused tile kernels
+template <typename T>
+struct TileArgs {
+    const T* zin;      // iterate read (PRE: unless zero_init; POST: before the correction)
+    T* zout;           // iterate written; never the array zin points to, because
+                       // neighbouring tiles read zin as their halo concurrently
+    const T* b;
+    T* bc;             // PRE: coarse source out
+    const T* zc;       // POST: coarse correction in
+    int zero_init;     // PRE: z starts from zero (coarse levels)
+    int norm;          // POST: residual norm + decision
+    Reduce rd;
+    SolveCtl* ctl;
+    int use_cond;
+    cudaGraphConditionalHandle h;
+};
+
+template <int KIND, int MODE, int NS>
+struct TileShape {
+    static constexpr int NCOL = KIND == 0 ? 2 : 4;
+    static constexpr int K = NS * NCOL;               // colour phases
+    static constexpr int ZH = (MODE == 0 && KIND == 1) ? K + 2 : K + 1;  // z halo
+    static constexpr int BH = ZH - 1;                 // b halo
+};
+
+/** Tile shape: TX x TY interior points per CTA of NT threads. The large
+ * shape serves the finest levels; the small one keeps coarser multi-CTA
+ * levels spread over all SMs. */
+template <typename T, int KIND, int SMALL>
+struct TileDims;
+template <> struct TileDims<double, 0, 0> { static constexpr int TX = 64, TY = 16, NT = 512; };
+template <> struct TileDims<float, 0, 0> { static constexpr int TX = 64, TY = 32, NT = 512; };
+template <> struct TileDims<double, 1, 0> { static constexpr int TX = 64, TY = 32, NT = 512; };
+template <> struct TileDims<float, 1, 0> { static constexpr int TX = 64, TY = 32, NT = 512; };
+template <typename T, int KIND> struct TileDims<T, KIND, 1> { static constexpr int TX = 32, TY = 16, NT = 256; };
+
+template <typename T, int KIND, int MODE, int NS, int SMALL>
+constexpr size_t tile_smem() {
+    using S = TileShape<KIND, MODE, NS>;
+    using D = TileDims<T, KIND, SMALL>;
+    size_t zb = size_t(D::TX + 2 * S::ZH) * (D::TY + 2 * S::ZH);
+    size_t bb = size_t(D::TX + 2 * S::BH) * (D::TY + 2 * S::BH);
+    size_t rb = (MODE == 0 && KIND == 1) ? size_t(D::TX + 2) * (D::TY + 2) : 0;
+    return (zb + bb + rb) * sizeof(T);
+}
+
+/** One sweep colour over the points of region [xs,xs+W) x [ys,ys+H) that lie
+ * in the grid. Inlined into a fully unrolled phase loop, so W and H are
+ * compile-time constants there. */
+template <typename T, int KIND, int NT, class OP>
+__device__ __forceinline__ void tile_phase(const OP& c, T* zt, const T* bt, int ZW, int zx, int zy, int BW, int bx,
+                                           int by, int color, int xs, int ys, int W, int H) {
+    const int M = op_m(c), N = op_n(c);
+    if (KIND == 0) {
+        const int half = (W + 1) >> 1, tot = H * half;
+#pragma unroll 4
+        for (int t = threadIdx.x; t < tot; t += NT) {
+            int row = t / half, c2 = t - row * half;
+            int j = ys + row;
+            int i = xs + 2 * c2 + ((color ^ (xs + j)) & 1);
+            if (i >= xs + W || i < 0 || i >= M || j < 0 || j >= N) continue;
+            T* w = zt + (i - zx) + ZW * (j - zy);
+            *w = op_relaxed(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
+        }
+    } else {
+        const int ci = color & 1, cj = color >> 1;
+        const int W2 = (W + 1) >> 1, H2 = (H + 1) >> 1, tot = W2 * H2;
+        const int pi = (ci ^ xs) & 1, pj = (cj ^ ys) & 1;
+#pragma unroll 4
+        for (int t = threadIdx.x; t < tot; t += NT) {
+            int jr = t / W2, ir = t - jr * W2;
+            int j = ys + 2 * jr + pj, i = xs + 2 * ir + pi;
+            if (i >= xs + W || j >= ys + H || i < 0 || i >= M || j < 0 || j >= N) continue;
+            T* w = zt + (i - zx) + ZW * (j - zy);
+            *w = op_relaxed(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
+        }
     }
-    s = block_sum(s);
-    double total;
-    if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
 }
 
-template <typename T>
-__global__ void cc_apply(CCc<T> c, const T* __restrict__ z, T* __restrict__ y) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= c.m * c.n) return;
-    int j = k / c.m, i = k - j * c.m;
-    y[k] = c.d[cls(i, c.m)][cls(j, c.n)] * z[k] + cc_off(c, z, i, j);
+/** Loads a (W x H) window with origin (ox,oy) of a grid array into shared
+ * memory (zero outside the grid; with zc, adds the prolonged coarse
+ * correction). All loads of a thread are issued before any store so they
+ * are in flight together. */
+template <typename T, int W, int H, int NT, int MODE, class OP>
+__device__ __forceinline__ void tile_load(const OP& c, T* dst, const T* src, const T* zc, int ox, int oy,
+                                          bool zero) {
+    constexpr int NL = (W * H + NT - 1) / NT;
+    const int M = op_m(c), N = op_n(c);
+    T v[NL];
+#pragma unroll
+    for (int q = 0; q < NL; q++) {
+        int t = threadIdx.x + q * NT;
+        int jj = t / W, ii = t - jj * W;
+        int i = ox + ii, j = oy + jj;
+        bool in = t < W * H && i >= 0 && i < M && j >= 0 && j < N;
+        v[q] = (in && !zero) ? src[i + M * j] : T(0);
+        if (MODE == 1 && in) v[q] += op_interp(c, zc, i, j);
+    }
+#pragma unroll
+    for (int q = 0; q < NL; q++) {
+        int t = threadIdx.x + q * NT;
+        if (t < W * H) dst[t] = v[q];
+    }
 }
 
-template <typename T>
-__global__ void cc_residual_out(CCc<T> c, const T* __restrict__ z, const T* __restrict__ b, T* __restrict__ r) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= c.m * c.n) return;
-    int j = k / c.m, i = k - j * c.m;
-    r[k] = cc_resid(c, z, b, i, j);
+template <typename T, int KIND, int MODE, int NS, int SMALL, class OP>
+__global__ void __launch_bounds__(TileDims<T, KIND, SMALL>::NT) mg_tile(OP c, TileArgs<T> a) {
+    using S = TileShape<KIND, MODE, NS>;
+    using D = TileDims<T, KIND, SMALL>;
+    constexpr int TX = D::TX, TY = D::TY, NT = D::NT, ZH = S::ZH, BH = S::BH, K = S::K, NCOL = S::NCOL;
+    constexpr int ZW = TX + 2 * ZH, ZHT = TY + 2 * ZH, BW = TX + 2 * BH, BHT = TY + 2 * BH;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* zt = reinterpret_cast<T*>(sm_raw);
+    T* bt = zt + ZW * ZHT;
+    T* rt = bt + BW * BHT;
+    const int M = op_m(c), N = op_n(c);
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zx = x0 - ZH, zy = y0 - ZH, bx = x0 - BH, by = y0 - BH;
+    tile_load<T, ZW, ZHT, NT, MODE>(c, zt, a.zin, a.zc, zx, zy, MODE == 0 && a.zero_init);
+    tile_load<T, BW, BHT, NT, 0>(c, bt, a.b, nullptr, bx, by, false);
+    __syncthreads();
+#pragma unroll
+    for (int k = 1; k <= K; k++) {
+        const int ph = (k - 1) % NCOL;
+        const int color = MODE == 0 ? ph : NCOL - 1 - ph;
+        const int r = ZH - k;
+        tile_phase<T, KIND, NT>(c, zt, bt, ZW, zx, zy, BW, bx, by, color, x0 - r, y0 - r, TX + 2 * r, TY + 2 * r);
+        __syncthreads();
+    }
+    // interior back to global memory
+#pragma unroll 4
+    for (int t = threadIdx.x; t < TX * TY; t += NT) {
+        int jj = t / TX, ii = t - jj * TX;
+        int i = x0 + ii, j = y0 + jj;
+        if (i < M && j < N) a.zout[i + M * j] = zt[(i - zx) + ZW * (j - zy)];
+    }
+    if (MODE == 0) {
+        if (KIND == 0) {
+            const int mc = M >> 1, nc = N >> 1;
+            for (int t = threadIdx.x; t < (TX / 2) * (TY / 2); t += NT) {
+                int q = t / (TX / 2);
+                int I = x0 / 2 + (t - q * (TX / 2)), J = y0 / 2 + q;
+                if (I >= mc || J >= nc) continue;
+                T s = 0;
+#pragma unroll
+                for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+                    for (int di = 0; di < 2; di++) {
+                        int i = 2 * I + di, j = 2 * J + dj;
+                        const T* w = zt + (i - zx) + ZW * (j - zy);
+                        s += op_resid(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
+                    }
+                a.bc[I + mc * J] = T(0.25) * s;
+            }
+        } else {
+            constexpr int RW = TX + 2, RH = TY + 2;
+            for (int t = threadIdx.x; t < RW * RH; t += NT) {
+                int jj = t / RW, ii = t - jj * RW;
+                int i = x0 - 1 + ii, j = y0 - 1 + jj;
+                T v = 0;
+                if (i >= 0 && i < M && j >= 0 && j < N) {
+                    const T* w = zt + (i - zx) + ZW * (j - zy);
+                    v = op_resid(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
+                }
+                rt[t] = v;
+            }
+            __syncthreads();
+            const int Mc = (M - 1) / 2 + 1, Nc = (N - 1) / 2 + 1;
+            for (int t = threadIdx.x; t < (TX / 2) * (TY / 2); t += NT) {
+                int q = t / (TX / 2);
+                int I = x0 / 2 + (t - q * (TX / 2)), J = y0 / 2 + q;
+                if (I >= Mc || J >= Nc) continue;
+                a.bc[I + Mc * J] = fem_restrict_at(M, N, rt, RW, x0 - 1, y0 - 1, I, J);
+            }
+        }
+    } else if (a.norm) {
+        double s = 0;
+        for (int t = threadIdx.x; t < TX * TY; t += NT) {
+            int jj = t / TX, ii = t - jj * TX;
+            int i = x0 + ii, j = y0 + jj;
+            if (i < M && j < N) {
+                const T* w = zt + (i - zx) + ZW * (j - zy);
+                double r = double(op_resid(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j));
+                s += r * r;
+            }
+        }
+        s = block_sum(s);
+        double total;
+        if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
+    }
 }
 
-/** The remaining levels of a cell-centred V-cycle inside one CTA: level 0
- * of the descriptor reads b (and z unless zero_init) from global memory and
- * writes z back; every array lives in shared memory. */
+// ---------------------------------------------------- CTA-resident levels
 template <typename T>
 struct CCStack {
     int nl;
@@ -269,11 +455,36 @@ struct CCStack {
 };
 
 template <typename T>
-__device__ void cta_cc_sweep(const CCc<T>& c, T* z, const T* b, int color) {
-    int tot = c.m * c.n;
-    for (int k = threadIdx.x; k < tot; k += blockDim.x) {
-        int j = k / c.m, i = k - j * c.m;
-        if (((i + j) & 1) == color) cc_relax(c, z, b, i, j);
+struct FEMStack {
+    int nl;
+    FEMc<T> lv[MAXLEV];
+    int off[MAXLEV];     // z_l, then b_l, then r_l
+    int nu1, nu2, ncoarse;
+};
+
+/** One colour of a whole-level sweep inside the CTA (colour-indexed). */
+template <typename T>
+__device__ void cta_sweep(const CCc<T>& c, T* z, const T* b, int color) {
+    const int half = (c.m + 1) >> 1, tot = half * c.n;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        int j = t / half;
+        int i = 2 * (t - j * half) + ((color ^ j) & 1);
+        if (i >= c.m) continue;
+        T* w = z + i + c.m * j;
+        *w = op_relaxed(c, w, b[i + c.m * j], c.m, i, j);
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ void cta_sweep(const FEMc<T>& c, T* z, const T* b, int color) {
+    const int ci = color & 1, cj = color >> 1;
+    const int W2 = (c.M - ci + 1) >> 1, H2 = (c.N - cj + 1) >> 1, tot = W2 * H2;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        int q = t / W2;
+        int i = ci + 2 * (t - q * W2), j = cj + 2 * q;
+        T* w = z + i + c.M * j;
+        *w = op_relaxed(c, w, b[i + c.M * j], c.M, i, j);
     }
     __syncthreads();
 }
@@ -287,54 +498,48 @@ __global__ void __launch_bounds__(CTA_THREADS) cc_cta_cycle(CCStack<T> st, const
         const CCc<T>& c0 = st.lv[0];
         T* z = sm + st.off[0];
         T* b = z + c0.m * c0.n;
-        int tot = c0.m * c0.n;
-        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
+        for (int k = threadIdx.x; k < c0.m * c0.n; k += blockDim.x) {
             b[k] = gb[k];
             z[k] = zero_init ? T(0) : gz[k];
         }
+        for (int l = 1; l < st.nl; l++) {
+            T* zl = sm + st.off[l];
+            for (int k = threadIdx.x; k < st.lv[l].m * st.lv[l].n; k += blockDim.x) zl[k] = T(0);
+        }
     }
     __syncthreads();
-    // descend
     for (int l = 0; l < st.nl - 1; l++) {
         const CCc<T>& c = st.lv[l];
         T* z = sm + st.off[l];
         T* b = z + c.m * c.n;
-        if (l > 0) {
-            for (int k = threadIdx.x; k < c.m * c.n; k += blockDim.x) z[k] = T(0);
-            __syncthreads();
-        }
         for (int s = 0; s < st.nu1; s++) {
-            cta_cc_sweep(c, z, b, 0);
-            cta_cc_sweep(c, z, b, 1);
+            cta_sweep(c, z, b, 0);
+            cta_sweep(c, z, b, 1);
         }
         const CCc<T>& cc = st.lv[l + 1];
         T* bcn = sm + st.off[l + 1] + cc.m * cc.n;
         for (int k = threadIdx.x; k < cc.m * cc.n; k += blockDim.x) {
             int J = k / cc.m, I = k - J * cc.m;
-            int i = 2 * I, j = 2 * J;
-            T s = cc_resid(c, z, b, i, j) + cc_resid(c, z, b, i + 1, j) + cc_resid(c, z, b, i, j + 1) +
-                  cc_resid(c, z, b, i + 1, j + 1);
+            T s = 0;
+            for (int dj = 0; dj < 2; dj++)
+                for (int di = 0; di < 2; di++) {
+                    int i = 2 * I + di, j = 2 * J + dj;
+                    s += op_resid(c, z + i + c.m * j, b[i + c.m * j], c.m, i, j);
+                }
             bcn[k] = T(0.25) * s;
         }
         __syncthreads();
     }
-    // coarsest: plain sweeps from zero
     {
-        int l = st.nl - 1;
-        const CCc<T>& c = st.lv[l];
-        T* z = sm + st.off[l];
+        const CCc<T>& c = st.lv[st.nl - 1];
+        T* z = sm + st.off[st.nl - 1];
         T* b = z + c.m * c.n;
-        if (l > 0) {
-            for (int k = threadIdx.x; k < c.m * c.n; k += blockDim.x) z[k] = T(0);
-            __syncthreads();
-        }
-        int ns = (l > 0) ? st.ncoarse : st.nu1 + st.nu2;
+        int ns = st.nl > 1 ? st.ncoarse : st.nu1 + st.nu2;
         for (int s = 0; s < ns; s++) {
-            cta_cc_sweep(c, z, b, 0);
-            cta_cc_sweep(c, z, b, 1);
+            cta_sweep(c, z, b, 0);
+            cta_sweep(c, z, b, 1);
         }
     }
-    // ascend
     for (int l = st.nl - 2; l >= 0; l--) {
         const CCc<T>& c = st.lv[l];
         T* z = sm + st.off[l];
@@ -342,12 +547,12 @@ __global__ void __launch_bounds__(CTA_THREADS) cc_cta_cycle(CCStack<T> st, const
         const T* zc = sm + st.off[l + 1];
         for (int k = threadIdx.x; k < c.m * c.n; k += blockDim.x) {
             int j = k / c.m, i = k - j * c.m;
-            z[k] += cc_interp(c, zc, c.m >> 1, c.n >> 1, i, j);
+            z[k] += cc_interp(c, zc, i, j);
         }
         __syncthreads();
         for (int s = 0; s < st.nu2; s++) {
-            cta_cc_sweep(c, z, b, 1);
-            cta_cc_sweep(c, z, b, 0);
+            cta_sweep(c, z, b, 1);
+            cta_sweep(c, z, b, 0);
         }
     }
     {
@@ -355,167 +560,6 @@ __global__ void __launch_bounds__(CTA_THREADS) cc_cta_cycle(CCStack<T> st, const
         const T* z = sm + st.off[0];
         for (int k = threadIdx.x; k < c0.m * c0.n; k += blockDim.x) gz[k] = z[k];
     }
-}
-
-// ------------------------------------------------------------- FEM ops
-template <typename T>
-struct FEMc {
-    int M, N;
-    T fm, fey, hey, fex, hex, fc;
-    T d[3][3], invd[3][3];
-};
-
-/** mul_a of mgs_fem.cc:32-53 on a grid array with pitch M. */
-template <typename T>
-__device__ __forceinline__ T fem_off(const FEMc<T>& c, const T* z, int i, int j) {
-    if (j == 0) return T(0);
-    const int M = c.M;
-    const T* w = z + i + M * j;
-    const T* wm = w - M;
-    if (j == c.N - 1) {
-        if (i == 0) return c.fc * wm[1] + c.hey * (*wm) + c.hex * w[1];
-        if (i == M - 1) return c.fc * wm[-1] + c.hey * (*wm) + c.hex * w[-1];
-        return c.fc * (wm[-1] + wm[1]) + c.fey * (*wm) + c.hex * (w[-1] + w[1]);
-    }
-    if (i == 0) return c.fc * (wm[1] + w[M + 1]) + c.hey * (*wm + w[M]) + c.fex * w[1];
-    if (i == M - 1) return c.fc * (wm[-1] + w[M - 1]) + c.hey * (*wm + w[M]) + c.fex * w[-1];
-    return c.fc * (wm[-1] + wm[1] + w[M - 1] + w[M + 1]) + c.fey * (*wm + w[M]) + c.fex * (w[-1] + w[1]);
-}
-
-template <typename T>
-__device__ __forceinline__ T fem_resid(const FEMc<T>& c, const T* z, const T* b, int i, int j) {
-    int ij = i + c.M * j;
-    return b[ij] - c.d[cls(i, c.M)][cls(j, c.N)] * z[ij] - fem_off(c, z, i, j);
-}
-
-template <typename T>
-__device__ __forceinline__ void fem_relax(const FEMc<T>& c, T* z, const T* b, int i, int j) {
-    int ij = i + c.M * j;
-    z[ij] = (b[ij] - fem_off(c, z, i, j)) * c.invd[cls(i, c.M)][cls(j, c.N)];
-}
-
-/** P^T r at coarse node (I,J); zero on the Dirichlet bottom row. */
-template <typename T>
-__device__ __forceinline__ T fem_restrict_at(int M, int N, const T* r, int I, int J) {
-    if (J == 0) return T(0);
-    T s = 0;
-    for (int dj = -1; dj <= 1; dj++) {
-        int j = 2 * J + dj;
-        if (j < 0 || j >= N) continue;
-        T wy = dj == 0 ? T(1) : T(0.5);
-        for (int di = -1; di <= 1; di++) {
-            int i = 2 * I + di;
-            if (i < 0 || i >= M) continue;
-            T wx = di == 0 ? T(1) : T(0.5);
-            s += wx * wy * r[i + M * j];
-        }
-    }
-    return s;
-}
-
-/** Bilinear prolongation of node-centred corrections to fine node (i,j). */
-template <typename T>
-__device__ __forceinline__ T fem_interp(const T* zc, int Mc, int i, int j) {
-    int I = i >> 1, J = j >> 1;
-    bool ox = i & 1, oy = j & 1;
-    T c00 = zc[I + Mc * J];
-    if (!ox && !oy) return c00;
-    if (ox && !oy) return T(0.5) * (c00 + zc[I + 1 + Mc * J]);
-    if (!ox && oy) return T(0.5) * (c00 + zc[I + Mc * (J + 1)]);
-    return T(0.25) * (c00 + zc[I + 1 + Mc * J] + zc[I + Mc * (J + 1)] + zc[I + 1 + Mc * (J + 1)]);
-}
-
-template <typename T>
-__global__ void fem_color_sweep(FEMc<T> c, T* __restrict__ z, const T* __restrict__ b, int ci, int cj) {
-    int mx = (c.M - ci + 1) >> 1, my = (c.N - cj + 1) >> 1;
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= mx * my) return;
-    int q = k / mx;
-    int i = ci + 2 * (k - q * mx), j = cj + 2 * q;
-    fem_relax(c, z, b, i, j);
-}
-
-template <typename T>
-__global__ void fem_residual_k(FEMc<T> c, const T* __restrict__ z, const T* __restrict__ b, T* __restrict__ r) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= c.M * c.N) return;
-    int j = k / c.M, i = k - j * c.M;
-    r[k] = fem_resid(c, z, b, i, j);
-}
-
-template <typename T>
-__global__ void fem_restrict_k(int M, int N, const T* __restrict__ r, int Mc, int Nc, T* __restrict__ bc) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= Mc * Nc) return;
-    int J = k / Mc, I = k - J * Mc;
-    bc[k] = fem_restrict_at(M, N, r, I, J);
-}
-
-template <typename T>
-__global__ void fem_prolong_add(int M, int N, T* __restrict__ z, int Mc, const T* __restrict__ zc) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= M * N) return;
-    int j = k / M, i = k - j * M;
-    if (j == 0) return;
-    z[k] += fem_interp(zc, Mc, i, j);
-}
-
-template <typename T>
-__global__ void fem_resid_norm(FEMc<T> c, const T* __restrict__ z, const T* __restrict__ b, Reduce rd,
-                               SolveCtl* ctl, int count_cycle, int use_cond, cudaGraphConditionalHandle h) {
-    double s = 0;
-    int tot = c.M * c.N;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
-        int j = k / c.M, i = k - j * c.M;
-        double r = double(fem_resid(c, z, b, i, j));
-        s += r * r;
-    }
-    s = block_sum(s);
-    double total;
-    if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
-}
-
-__global__ void fem_resid_to32(FEMc<double> c, const double* __restrict__ z, const double* __restrict__ b,
-                               float* __restrict__ r32, Reduce rd, SolveCtl* ctl, int count_cycle,
-                               int use_cond, cudaGraphConditionalHandle h) {
-    double s = 0;
-    int tot = c.M * c.N;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
-        int j = k / c.M, i = k - j * c.M;
-        double r = fem_resid(c, z, b, i, j);
-        r32[k] = float(r);
-        s += r * r;
-    }
-    s = block_sum(s);
-    double total;
-    if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
-}
-
-template <typename T>
-__global__ void fem_apply(FEMc<T> c, const T* __restrict__ z, T* __restrict__ y) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= c.M * c.N) return;
-    int j = k / c.M, i = k - j * c.M;
-    y[k] = c.d[cls(i, c.M)][cls(j, c.N)] * z[k] + fem_off(c, z, i, j);
-}
-
-template <typename T>
-struct FEMStack {
-    int nl;
-    FEMc<T> lv[MAXLEV];
-    int off[MAXLEV];     // z_l, then b_l, then r_l
-    int nu1, nu2, ncoarse;
-};
-
-template <typename T>
-__device__ void cta_fem_sweep(const FEMc<T>& c, T* z, const T* b, int color) {
-    int ci = color & 1, cj = color >> 1;
-    int tot = c.M * c.N;
-    for (int k = threadIdx.x; k < tot; k += blockDim.x) {
-        int j = k / c.M, i = k - j * c.M;
-        if ((i & 1) == ci && (j & 1) == cj) fem_relax(c, z, b, i, j);
-    }
-    __syncthreads();
 }
 
 template <typename T>
@@ -531,6 +575,10 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
             b[k] = gb[k];
             z[k] = zero_init ? T(0) : gz[k];
         }
+        for (int l = 1; l < st.nl; l++) {
+            T* zl = sm + st.off[l];
+            for (int k = threadIdx.x; k < st.lv[l].M * st.lv[l].N; k += blockDim.x) zl[k] = T(0);
+        }
     }
     __syncthreads();
     for (int l = 0; l < st.nl - 1; l++) {
@@ -539,37 +587,28 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
         T* z = sm + st.off[l];
         T* b = z + tot;
         T* r = b + tot;
-        if (l > 0) {
-            for (int k = threadIdx.x; k < tot; k += blockDim.x) z[k] = T(0);
-            __syncthreads();
-        }
         for (int s = 0; s < st.nu1; s++)
-            for (int q = 0; q < 4; q++) cta_fem_sweep(c, z, b, q);
+            for (int q = 0; q < 4; q++) cta_sweep(c, z, b, q);
         for (int k = threadIdx.x; k < tot; k += blockDim.x) {
             int j = k / c.M, i = k - j * c.M;
-            r[k] = fem_resid(c, z, b, i, j);
+            r[k] = op_resid(c, z + k, b[k], c.M, i, j);
         }
         __syncthreads();
         const FEMc<T>& cc = st.lv[l + 1];
         T* bcn = sm + st.off[l + 1] + cc.M * cc.N;
         for (int k = threadIdx.x; k < cc.M * cc.N; k += blockDim.x) {
             int J = k / cc.M, I = k - J * cc.M;
-            bcn[k] = fem_restrict_at(c.M, c.N, r, I, J);
+            bcn[k] = fem_restrict_at(c.M, c.N, r, c.M, 0, 0, I, J);
         }
         __syncthreads();
     }
     {
-        int l = st.nl - 1;
-        const FEMc<T>& c = st.lv[l];
-        T* z = sm + st.off[l];
+        const FEMc<T>& c = st.lv[st.nl - 1];
+        T* z = sm + st.off[st.nl - 1];
         T* b = z + c.M * c.N;
-        if (l > 0) {
-            for (int k = threadIdx.x; k < c.M * c.N; k += blockDim.x) z[k] = T(0);
-            __syncthreads();
-        }
-        int ns = (l > 0) ? st.ncoarse : st.nu1 + st.nu2;
+        int ns = st.nl > 1 ? st.ncoarse : st.nu1 + st.nu2;
         for (int s = 0; s < ns; s++)
-            for (int q = 0; q < 4; q++) cta_fem_sweep(c, z, b, q);
+            for (int q = 0; q < 4; q++) cta_sweep(c, z, b, q);
     }
     for (int l = st.nl - 2; l >= 0; l--) {
         const FEMc<T>& c = st.lv[l];
@@ -579,11 +618,11 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
         const T* zc = sm + st.off[l + 1];
         for (int k = threadIdx.x; k < tot; k += blockDim.x) {
             int j = k / c.M, i = k - j * c.M;
-            if (j > 0) z[k] += fem_interp(zc, st.lv[l + 1].M, i, j);
+            z[k] += fem_interp(c, zc, i, j);
         }
         __syncthreads();
         for (int s = 0; s < st.nu2; s++)
-            for (int q = 3; q >= 0; q--) cta_fem_sweep(c, z, b, q);
+            for (int q = 3; q >= 0; q--) cta_sweep(c, z, b, q);
     }
     {
         const FEMc<T>& c0 = st.lv[0];
@@ -592,10 +631,81 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
     }
 }
 
-// ------------------------------------------------------------ misc kernels
-__global__ void norm2_kernel(const double* __restrict__ x, int n, Reduce rd, SolveCtl* ctl) {
+// ------------------------------------------------------- whole-grid kernels
+template <class OP>
+__device__ __forceinline__ void grid_ij(const OP& c, long k, int& i, int& j) {
+    j = int(k / op_m(c));
+    i = int(k - long(j) * op_m(c));
+}
+
+/** ||b - A z||^2 accumulated in FP64, then the solve decision. */
+template <typename T, class OP>
+__global__ void resid_norm_k(OP c, const T* __restrict__ z, const T* __restrict__ b, Reduce rd, SolveCtl* ctl,
+                             int count_cycle, int use_cond, cudaGraphConditionalHandle h) {
     double s = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) s += x[k] * x[k];
+    const long tot = long(op_m(c)) * op_n(c);
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
+        int i, j;
+        grid_ij(c, k, i, j);
+        double r = double(op_resid(c, z + k, b[k], op_m(c), i, j));
+        s += r * r;
+    }
+    s = block_sum(s);
+    double total;
+    if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
+}
+
+/** FP64 residual of an FP64 iterate written as FP32 (a refinement step),
+ * with its FP64 norm and the solve decision. */
+template <class OP>
+__global__ void resid_to32_k(OP c, const double* __restrict__ z, const double* __restrict__ b,
+                             float* __restrict__ r32, Reduce rd, SolveCtl* ctl, int count_cycle, int use_cond,
+                             cudaGraphConditionalHandle h) {
+    double s = 0;
+    const long tot = long(op_m(c)) * op_n(c);
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
+        int i, j;
+        grid_ij(c, k, i, j);
+        double r = op_resid(c, z + k, b[k], op_m(c), i, j);
+        r32[k] = float(r);
+        s += r * r;
+    }
+    s = block_sum(s);
+    double total;
+    if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
+}
+
+template <typename T, class OP>
+__global__ void apply_k(OP c, const T* __restrict__ z, T* __restrict__ y) {
+    const long tot = long(op_m(c)) * op_n(c);
+    long k = blockIdx.x * long(blockDim.x) + threadIdx.x;
+    if (k >= tot) return;
+    int i, j;
+    grid_ij(c, k, i, j);
+    y[k] = c.d[cls(i, op_m(c))][cls(j, op_n(c))] * z[k] + op_off(c, z + k, op_m(c), i, j);
+}
+
+template <typename T, class OP>
+__global__ void resid_out_k(OP c, const T* __restrict__ z, const T* __restrict__ b, T* __restrict__ r, Reduce rd,
+                            double* out) {
+    double s = 0;
+    const long tot = long(op_m(c)) * op_n(c);
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
+        int i, j;
+        grid_ij(c, k, i, j);
+        T v = op_resid(c, z + k, b[k], op_m(c), i, j);
+        if (r) r[k] = v;
+        s += double(v) * double(v);
+    }
+    s = block_sum(s);
+    double total;
+    if (grid_sum(s, rd, &total) && threadIdx.x == 0) *out = sqrt(total);
+}
+
+__global__ void norm2_kernel(const double* __restrict__ x, long n, Reduce rd, SolveCtl* ctl) {
+    double s = 0;
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < n; k += long(gridDim.x) * blockDim.x)
+        s += x[k] * x[k];
     s = block_sum(s);
     double total;
     if (grid_sum(s, rd, &total) && threadIdx.x == 0) {
@@ -608,43 +718,19 @@ __global__ void norm2_kernel(const double* __restrict__ x, int n, Reduce rd, Sol
 
 /** If ||b|| = 0 the solution is z = 0 (the shim and this library agree on
  * that convention); zero z once the norm is known. */
-__global__ void zero_if_b_zero(double* __restrict__ z, int n, const SolveCtl* ctl) {
+__global__ void zero_if_b_zero(double* __restrict__ z, long n, const SolveCtl* ctl) {
     if (ctl->bnorm2 != 0.) return;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) z[k] = 0.;
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < n; k += long(gridDim.x) * blockDim.x) z[k] = 0.;
 }
 
-__global__ void add_f32_to_f64(double* __restrict__ z, const float* __restrict__ e, int n) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void add_f32_to_f64(double* __restrict__ z, const float* __restrict__ e, long n) {
+    long k = blockIdx.x * long(blockDim.x) + threadIdx.x;
     if (k < n) z[k] += double(e[k]);
-}
-
-__global__ void norm_result(const Reduce rd, double* out) {}
-
-/** Writes the final residual norm of a standalone residual computation. */
-template <typename T>
-__global__ void resid_norm_plain(int kind, CCc<T> cc, FEMc<T> fc, const T* z, const T* b, T* r, Reduce rd,
-                                 double* out) {
-    double s = 0;
-    int tot = kind == VDI_MG_FEM ? fc.M * fc.N : cc.m * cc.n;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
-        double v;
-        if (kind == VDI_MG_FEM) {
-            int j = k / fc.M, i = k - j * fc.M;
-            v = double(fem_resid(fc, z, b, i, j));
-        } else {
-            int j = k / cc.m, i = k - j * cc.m;
-            v = double(cc_resid(cc, z, b, i, j));
-        }
-        if (r) r[k] = T(v);
-        s += v * v;
-    }
-    s = block_sum(s);
-    double total;
-    if (grid_sum(s, rd, &total) && threadIdx.x == 0) *out = sqrt(total);
 }
 
 // =================================================================== host
 static inline int nblk(long n, int t = 256) { return int((n + t - 1) / t); }
+static inline int rblocks(long n) { return std::max(1, std::min(MAX_PARTIALS, nblk(n, 256))); }
 
 /** Per-level description in double precision, converted per precision. */
 struct LevelD {
@@ -654,11 +740,35 @@ struct LevelD {
     signed char gL, gR, gD, gU;
 };
 
+template <typename T, int KIND, int MODE, class OP>
+static void launch_tile(cudaStream_t s, const OP& c, const TileArgs<T>& a, int M, int N) {
+    using DL = TileDims<T, KIND, 0>;
+    using DS = TileDims<T, KIND, 1>;
+    long big = long((M + DL::TX - 1) / DL::TX) * ((N + DL::TY - 1) / DL::TY);
+    if (big >= 1024) {
+        dim3 grid((M + DL::TX - 1) / DL::TX, (N + DL::TY - 1) / DL::TY);
+        mg_tile<T, KIND, MODE, 2, 0, OP><<<grid, DL::NT, tile_smem<T, KIND, MODE, 2, 0>(), s>>>(c, a);
+    } else {
+        dim3 grid((M + DS::TX - 1) / DS::TX, (N + DS::TY - 1) / DS::TY);
+        mg_tile<T, KIND, MODE, 2, 1, OP><<<grid, DS::NT, tile_smem<T, KIND, MODE, 2, 1>(), s>>>(c, a);
+    }
+}
+
+template <typename T, int KIND, int MODE, class OP>
+static cudaError_t tile_attr() {
+    cudaError_t e = cudaFuncSetAttribute(mg_tile<T, KIND, MODE, 2, 0, OP>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(tile_smem<T, KIND, MODE, 2, 0>()));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(mg_tile<T, KIND, MODE, 2, 1, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(tile_smem<T, KIND, MODE, 2, 1>()));
+}
+
 class MG {
   public:
     int kind = 0;
     int m = 0, n = 0;      // fine grid of the problem class (cells or nodes)
-    double c1 = 0, c2 = 0; // dx,dy (MAC/FEM) or vfx,vfy (viscous)
+    double c1 = 0, c2 = 0; // xxsp,yysp (MAC), dx,dy (FEM) or vfx,vfy (viscous)
     int x_sym = 0;
     std::vector<LevelD> lv;
     FEMOp fop{};
@@ -666,8 +776,8 @@ class MG {
     int nmulti64 = 0, nmulti32 = 0;
     size_t smem64 = 0, smem32 = 0;
     // device buffers: index l holds level l (level 0 of z64/b64 is the caller's)
-    std::vector<double*> z64, b64, r64;
-    std::vector<float*> z32, b32, r32;
+    std::vector<double*> z64, b64, t64;
+    std::vector<float*> z32, b32, t32;   // t: scratch iterate of each tiled level
     Reduce rd;
     SolveCtl* ctl = nullptr;
     int nu1 = 2, nu2 = 2;
@@ -679,16 +789,17 @@ class MG {
     void release() {
         for (auto p : z64) if (p) cudaFree(p);
         for (auto p : b64) if (p) cudaFree(p);
-        for (auto p : r64) if (p) cudaFree(p);
         for (auto p : z32) if (p) cudaFree(p);
         for (auto p : b32) if (p) cudaFree(p);
-        for (auto p : r32) if (p) cudaFree(p);
-        z64.clear(); b64.clear(); r64.clear(); z32.clear(); b32.clear(); r32.clear();
+        for (auto p : t64) if (p) cudaFree(p);
+        for (auto p : t32) if (p) cudaFree(p);
+        z64.clear(); b64.clear(); z32.clear(); b32.clear(); t64.clear(); t32.clear();
         reduce_free(rd);
         if (ctl) cudaFree(ctl);
         ctl = nullptr;
     }
 
+    bool fem() const { return kind == VDI_MG_FEM; }
     long size(int l) const { return long(lv[l].m) * lv[l].n; }
 
     /** Diagonals and couplings of level l, matching the problem classes'
@@ -703,11 +814,10 @@ class MG {
                 double v;
                 if (kind == VDI_MG_MAC) {
                     double xp = a == 1 ? -2 * kx : -kx;
-                    if (L.m == 1) xp = -kx;
                     double yp = b == 0 ? -3 * ky : (b == 1 ? -2 * ky : -ky);
                     v = xp + yp;
                 } else {
-                    double yp = b == 0 ? vfy_part(ky, true) : 2 * ky;
+                    double yp = b == 0 ? ky : 2 * ky;
                     if (x_sym) {
                         double xp = a == 0 ? (horiz ? 3 * kx : kx) : 2 * kx;
                         v = 1 + xp + yp;
@@ -724,7 +834,6 @@ class MG {
             L.gR = 0; L.gD = 1; L.gU = 0;
         }
     }
-    static double vfy_part(double ky, bool bottom) { return bottom ? ky : 2 * ky; }
 
     void fill_fem(LevelD& L) {
         for (int a = 0; a < 3; a++)
@@ -764,7 +873,7 @@ class MG {
 
     int build_levels() {
         lv.clear();
-        if (kind == VDI_MG_FEM) {
+        if (fem()) {
             double dydx = c2 / c1, dxdy = c1 / c2;
             // mgs_fem.cc:8-11
             fop.fm = 4. / 3. * (dxdy + dydx);
@@ -784,9 +893,7 @@ class MG {
                 N = (N - 1) / 2 + 1;
             }
         } else {
-            double kx, ky;
-            kx = c1;   // MAC: xxsp, yysp; viscous: vfx, vfy
-            ky = c2;
+            double kx = c1, ky = c2;   // MAC: xxsp, yysp; viscous: vfx, vfy
             int mm = m, nn = n;
             while (true) {
                 LevelD L{};
@@ -800,7 +907,7 @@ class MG {
         }
         nlev = int(lv.size());
         // the CTA-resident tail must fit in shared memory
-        int arrays = kind == VDI_MG_FEM ? 3 : 2;
+        int arrays = fem() ? 3 : 2;
         auto tail_bytes = [&](int from, size_t es) {
             size_t t = 0;
             for (int l = from; l < nlev; l++) t += size_t(arrays) * size(l) * es;
@@ -822,22 +929,23 @@ class MG {
     }
 
     int alloc() {
-        z64.assign(nlev, nullptr); b64.assign(nlev, nullptr); r64.assign(nlev, nullptr);
-        z32.assign(nlev, nullptr); b32.assign(nlev, nullptr); r32.assign(nlev, nullptr);
+        z64.assign(nlev, nullptr); b64.assign(nlev, nullptr);
+        z32.assign(nlev, nullptr); b32.assign(nlev, nullptr);
+        t64.assign(nlev, nullptr); t32.assign(nlev, nullptr);
         for (int l = 0; l < nlev; l++) {
             size_t s = size_t(size(l));
+            if (l < nmulti64) VDI_CUDA(cudaMalloc(&t64[l], s * 8));
+            if (l < nmulti32) VDI_CUDA(cudaMalloc(&t32[l], s * 4));
             if (l > 0 && l <= nmulti64) {
                 VDI_CUDA(cudaMalloc(&z64[l], s * 8));
                 VDI_CUDA(cudaMalloc(&b64[l], s * 8));
             }
-            if (kind == VDI_MG_FEM && l < nmulti64) VDI_CUDA(cudaMalloc(&r64[l], s * 8));
             if (l <= nmulti32) {
                 VDI_CUDA(cudaMalloc(&z32[l], s * 4));
                 VDI_CUDA(cudaMalloc(&b32[l], s * 4));
             }
-            if (kind == VDI_MG_FEM && l < nmulti32) VDI_CUDA(cudaMalloc(&r32[l], s * 4));
         }
-        VDI_TRY(reduce_alloc(rd, 1024));
+        VDI_TRY(reduce_alloc(rd, MAX_PARTIALS));
         VDI_CUDA(cudaMalloc(&ctl, sizeof(SolveCtl)));
         VDI_CUDA(cudaMemset(ctl, 0, sizeof(SolveCtl)));
         VDI_TRY(set_ctl_params(0, rtol, max_it));
@@ -849,21 +957,46 @@ class MG {
                                       int(CTA_SMEM_LIMIT)));
         VDI_CUDA(cudaFuncSetAttribute(fem_cta_cycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(CTA_SMEM_LIMIT)));
+        VDI_CUDA((tile_attr<double, 0, 0, CCc<double>>()));
+        VDI_CUDA((tile_attr<double, 0, 1, CCc<double>>()));
+        VDI_CUDA((tile_attr<float, 0, 0, CCc<float>>()));
+        VDI_CUDA((tile_attr<float, 0, 1, CCc<float>>()));
+        VDI_CUDA((tile_attr<double, 1, 0, FEMc<double>>()));
+        VDI_CUDA((tile_attr<double, 1, 1, FEMc<double>>()));
+        VDI_CUDA((tile_attr<float, 1, 0, FEMc<float>>()));
+        VDI_CUDA((tile_attr<float, 1, 1, FEMc<float>>()));
         return VDI_OK;
     }
 
-    int ncoarse_sweeps(int l) const {
-        long s = long(lv[l].m) + lv[l].n;
-        long v = 4 * s * s;
-        return int(std::min(400L, std::max(20L, v)));
+    /** Sweeps on the coarsest level: enough for its few points, few enough
+     * that the single-CTA cycle stays short. */
+    int ncoarse_sweeps() const {
+        int s = lv[nlev - 1].m + lv[nlev - 1].n;
+        return std::min(32, std::max(4, s));
     }
 
-    /** One V-cycle on level l (precision T). z/b are level-l arrays. */
     template <typename T>
-    int vcycle(cudaStream_t s, int l, const T* b, T* z, int nmulti, std::vector<T*>& zs,
-               std::vector<T*>& bs, std::vector<T*>& rs, size_t smem) {
+    TileArgs<T> targs(const T* zin, T* zout, const T* b) const {
+        TileArgs<T> a{};
+        a.zin = zin;
+        a.zout = zout;
+        a.b = b;
+        a.rd = rd;
+        a.ctl = ctl;
+        return a;
+    }
+
+    double* ztmp(int l, double*) { return t64[l]; }
+    float* ztmp(int l, float*) { return t32[l]; }
+
+    /** One V-cycle from level l (precision T); z/b are level-l arrays. When
+     * norm is set, level 0's POST kernel ends with the residual norm and the
+     * solve decision. */
+    template <typename T>
+    int vcycle(cudaStream_t s, int l, const T* b, T* z, int nmulti, std::vector<T*>& zs, std::vector<T*>& bs,
+               size_t smem, int zero_init, int norm, int use_cond, cudaGraphConditionalHandle h) {
         if (l == nmulti) {
-            if (kind == VDI_MG_FEM) {
+            if (fem()) {
                 FEMStack<T> st{};
                 st.nl = nlev - l;
                 int off = 0;
@@ -872,8 +1005,8 @@ class MG {
                     st.off[q] = off;
                     off += 3 * int(size(l + q));
                 }
-                st.nu1 = nu1; st.nu2 = nu2; st.ncoarse = ncoarse_sweeps(nlev - 1);
-                fem_cta_cycle<T><<<1, CTA_THREADS, smem, s>>>(st, b, z, l > 0);
+                st.nu1 = nu1; st.nu2 = nu2; st.ncoarse = ncoarse_sweeps();
+                fem_cta_cycle<T><<<1, CTA_THREADS, smem, s>>>(st, b, z, zero_init);
             } else {
                 CCStack<T> st{};
                 st.nl = nlev - l;
@@ -883,100 +1016,81 @@ class MG {
                     st.off[q] = off;
                     off += 2 * int(size(l + q));
                 }
-                st.nu1 = nu1; st.nu2 = nu2; st.ncoarse = ncoarse_sweeps(nlev - 1);
-                cc_cta_cycle<T><<<1, CTA_THREADS, smem, s>>>(st, b, z, l > 0);
+                st.nu1 = nu1; st.nu2 = nu2; st.ncoarse = ncoarse_sweeps();
+                cc_cta_cycle<T><<<1, CTA_THREADS, smem, s>>>(st, b, z, zero_init);
             }
             VDI_CUDA(cudaGetLastError());
             return VDI_OK;
         }
-        long N = size(l);
-        if (l > 0) VDI_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * N, s));
-        if (kind == VDI_MG_FEM) {
-            FEMc<T> c = femc<T>(l);
-            auto sweep = [&](int q) {
-                int ci = q & 1, cj = q >> 1;
-                long cnt = long((c.M - ci + 1) >> 1) * ((c.N - cj + 1) >> 1);
-                fem_color_sweep<T><<<nblk(cnt), 256, 0, s>>>(c, z, b, ci, cj);
-            };
-            for (int k = 0; k < nu1; k++)
-                for (int q = 0; q < 4; q++) sweep(q);
-            fem_residual_k<T><<<nblk(N), 256, 0, s>>>(c, z, b, rs[l]);
-            fem_restrict_k<T><<<nblk(size(l + 1)), 256, 0, s>>>(c.M, c.N, rs[l], lv[l + 1].m, lv[l + 1].n,
-                                                                 bs[l + 1]);
-            VDI_TRY(vcycle<T>(s, l + 1, bs[l + 1], zs[l + 1], nmulti, zs, bs, rs, smem));
-            fem_prolong_add<T><<<nblk(N), 256, 0, s>>>(c.M, c.N, z, lv[l + 1].m, zs[l + 1]);
-            for (int k = 0; k < nu2; k++)
-                for (int q = 3; q >= 0; q--) sweep(q);
-        } else {
-            CCc<T> c = ccc<T>(l);
-            int half = int(N / 2);
-            for (int k = 0; k < nu1; k++) {
-                cc_rb_sweep<T><<<nblk(half), 256, 0, s>>>(c, z, b, 0);
-                cc_rb_sweep<T><<<nblk(half), 256, 0, s>>>(c, z, b, 1);
-            }
-            cc_resid_restrict<T><<<nblk(size(l + 1)), 256, 0, s>>>(c, z, b, bs[l + 1]);
-            VDI_TRY(vcycle<T>(s, l + 1, bs[l + 1], zs[l + 1], nmulti, zs, bs, rs, smem));
-            cc_prolong_add<T><<<nblk(N), 256, 0, s>>>(c, z, zs[l + 1]);
-            for (int k = 0; k < nu2; k++) {
-                cc_rb_sweep<T><<<nblk(half), 256, 0, s>>>(c, z, b, 1);
-                cc_rb_sweep<T><<<nblk(half), 256, 0, s>>>(c, z, b, 0);
-            }
-        }
+        // PRE writes the level's scratch iterate, POST reads it and writes z
+        T* zs_tmp = ztmp(l, static_cast<T*>(nullptr));
+        TileArgs<T> a = targs<T>(z, zs_tmp, b);
+        a.zero_init = zero_init;
+        a.bc = bs[l + 1];
+        if (fem()) launch_tile<T, 1, 0>(s, femc<T>(l), a, lv[l].m, lv[l].n);
+        else launch_tile<T, 0, 0>(s, ccc<T>(l), a, lv[l].m, lv[l].n);
+        VDI_CUDA(cudaGetLastError());
+        VDI_TRY(vcycle<T>(s, l + 1, bs[l + 1], zs[l + 1], nmulti, zs, bs, smem, 1, 0, 0, 0));
+        TileArgs<T> p = targs<T>(zs_tmp, z, b);
+        p.zc = zs[l + 1];
+        p.norm = norm;
+        p.use_cond = use_cond;
+        p.h = h;
+        if (fem()) launch_tile<T, 1, 1>(s, femc<T>(l), p, lv[l].m, lv[l].n);
+        else launch_tile<T, 0, 1>(s, ccc<T>(l), p, lv[l].m, lv[l].n);
         VDI_CUDA(cudaGetLastError());
         return VDI_OK;
     }
 
-    int vcycle64(cudaStream_t s, const double* b, double* z) {
-        return vcycle<double>(s, 0, b, z, nmulti64, z64, b64, r64, smem64);
+    int vcycle64(cudaStream_t s, const double* b, double* z, int norm, int use_cond, cudaGraphConditionalHandle h) {
+        VDI_TRY(vcycle<double>(s, 0, b, z, nmulti64, z64, b64, smem64, 0, norm && nmulti64 > 0, use_cond, h));
+        if (norm && nmulti64 == 0) VDI_TRY(enqueue_resid_norm(s, b, z, 1, use_cond, h));
+        return VDI_OK;
     }
     int vcycle32(cudaStream_t s) {
-        return vcycle<float>(s, 0, b32[0], z32[0], nmulti32, z32, b32, r32, smem32);
+        return vcycle<float>(s, 0, b32[0], z32[0], nmulti32, z32, b32, smem32, 1, 0, 0, 0);
     }
 
-    int norm_blocks() const { return std::min(rd.max_blocks, std::max(1, nblk(size(0), 256))); }
-
-    /** Enqueue: residual norm of z + decision (FP64 path). */
     int enqueue_resid_norm(cudaStream_t s, const double* b, const double* z, int count_cycle, int use_cond,
                            cudaGraphConditionalHandle h) {
-        int nb = std::min(norm_blocks(), 4 * 148);
-        if (kind == VDI_MG_FEM)
-            fem_resid_norm<double><<<nb, 256, 0, s>>>(femc<double>(0), z, b, rd, ctl, count_cycle, use_cond, h);
+        int nb = rblocks(size(0));
+        if (fem())
+            resid_norm_k<double><<<nb, 256, 0, s>>>(femc<double>(0), z, b, rd, ctl, count_cycle, use_cond, h);
         else
-            cc_resid_norm<double><<<nb, 256, 0, s>>>(ccc<double>(0), z, b, rd, ctl, count_cycle, use_cond, h);
+            resid_norm_k<double><<<nb, 256, 0, s>>>(ccc<double>(0), z, b, rd, ctl, count_cycle, use_cond, h);
         VDI_CUDA(cudaGetLastError());
         return VDI_OK;
     }
 
     int enqueue_resid32(cudaStream_t s, const double* b, const double* z, int count_cycle, int use_cond,
                         cudaGraphConditionalHandle h) {
-        int nb = std::min(norm_blocks(), 4 * 148);
-        if (kind == VDI_MG_FEM)
-            fem_resid_to32<<<nb, 256, 0, s>>>(femc<double>(0), z, b, b32[0], rd, ctl, count_cycle, use_cond, h);
+        int nb = rblocks(size(0));
+        if (fem())
+            resid_to32_k<<<nb, 256, 0, s>>>(femc<double>(0), z, b, b32[0], rd, ctl, count_cycle, use_cond, h);
         else
-            cc_resid_to32<<<nb, 256, 0, s>>>(ccc<double>(0), z, b, b32[0], rd, ctl, count_cycle, use_cond, h);
+            resid_to32_k<<<nb, 256, 0, s>>>(ccc<double>(0), z, b, b32[0], rd, ctl, count_cycle, use_cond, h);
         VDI_CUDA(cudaGetLastError());
         return VDI_OK;
     }
 
     int enqueue_begin(cudaStream_t s, const double* b, double* z) {
-        int nb = std::min(norm_blocks(), 4 * 148);
-        norm2_kernel<<<nb, 256, 0, s>>>(b, int(size(0)), rd, ctl);
-        zero_if_b_zero<<<nblk(size(0)), 256, 0, s>>>(z, int(size(0)), ctl);
+        int nb = rblocks(size(0));
+        norm2_kernel<<<nb, 256, 0, s>>>(b, size(0), rd, ctl);
+        zero_if_b_zero<<<std::min(nb, 1184), 256, 0, s>>>(z, size(0), ctl);
         VDI_CUDA(cudaGetLastError());
         return VDI_OK;
     }
 
-    /** One iteration of the solve loop body (precision-dependent). */
+    /** One iteration of the solve loop body (precision-dependent); ends with
+     * the residual norm of the new iterate and the solve decision. */
     int enqueue_body(cudaStream_t s, const double* b, double* z, int precision, int use_cond,
                      cudaGraphConditionalHandle h) {
         if (precision == VDI_MG_MIXED) {
-            VDI_CUDA(cudaMemsetAsync(z32[0], 0, sizeof(float) * size(0), s));
             VDI_TRY(vcycle32(s));
-            add_f32_to_f64<<<nblk(size(0)), 256, 0, s>>>(z, z32[0], int(size(0)));
+            add_f32_to_f64<<<nblk(size(0)), 256, 0, s>>>(z, z32[0], size(0));
             VDI_TRY(enqueue_resid32(s, b, z, 1, use_cond, h));
         } else {
-            VDI_TRY(vcycle64(s, b, z));
-            VDI_TRY(enqueue_resid_norm(s, b, z, 1, use_cond, h));
+            VDI_TRY(vcycle64(s, b, z, 1, use_cond, h));
         }
         return VDI_OK;
     }
@@ -990,9 +1104,14 @@ class MG {
     int set_ctl_params(cudaStream_t s, double rt, int mx) {
         rtol = rt;
         max_it = mx;
-        // rtol and max_it sit at fixed offsets; write them with one copy
-        struct P { double rtol; int it; int max_it; } p{rt, 0, mx};
+        // rtol, it and max_it are consecutive in SolveCtl; write them together
+        struct P {
+            double rtol;
+            int it;
+            int max_it;
+        } p{rt, 0, mx};
         static_assert(offsetof(SolveCtl, rtol) + sizeof(double) == offsetof(SolveCtl, it), "layout");
+        static_assert(offsetof(SolveCtl, it) + sizeof(int) == offsetof(SolveCtl, max_it), "layout");
         VDI_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(ctl) + offsetof(SolveCtl, rtol), &p,
                                  sizeof(double) + 2 * sizeof(int), cudaMemcpyHostToDevice, s));
         VDI_CUDA(cudaStreamSynchronize(s));
@@ -1035,11 +1154,7 @@ SolveCtl* mg_ctl(MG* mg) { return mg->ctl; }
 int mg_kind(const MG* mg) { return mg->kind; }
 int mg_fine_size(const MG* mg) { return int(mg->size(0)); }
 
-int mg_configure(MG* mg, double rtol, int max_it) {
-    mg->rtol = rtol;
-    mg->max_it = max_it;
-    return mg->set_ctl_params(0, rtol, max_it);
-}
+int mg_configure(MG* mg, double rtol, int max_it) { return mg->set_ctl_params(0, rtol, max_it); }
 
 int mg_solve(MG* mg, cudaStream_t s, const double* b, double* z, double rtol, int max_it, int precision,
              int* vcycles, double* rel_res) {
@@ -1068,9 +1183,8 @@ int mg_solve(MG* mg, cudaStream_t s, const double* b, double* z, double rtol, in
 }
 
 int mg_solve_device(MG* mg, cudaStream_t s, const double* b, double* z, int precision) {
-    // Without a graph, loop control needs the host; this entry point records
-    // the conditional-node loop when s is capturing and otherwise falls back
-    // to the host-driven loop.
+    // Loop control needs the host unless the stream is capturing, in which
+    // case the loop becomes a conditional graph node.
     cudaStreamCaptureStatus cs;
     VDI_CUDA(cudaStreamIsCapturing(s, &cs));
     if (cs == cudaStreamCaptureStatusActive) return mg_record_graph_solve(mg, s, b, z, precision);
@@ -1114,18 +1228,16 @@ int mg_record_graph_solve(MG* mg, cudaStream_t s, const double* b, double* z, in
     return VDI_OK;
 }
 
-int mg_v_cycle(MG* mg, cudaStream_t s, const double* b, double* z) { return mg->vcycle64(s, b, z); }
+int mg_v_cycle(MG* mg, cudaStream_t s, const double* b, double* z) { return mg->vcycle64(s, b, z, 0, 0, 0); }
 
 int mg_residual(MG* mg, cudaStream_t s, const double* b, const double* z, double* r, double* norm) {
     double* d_out;
     VDI_CUDA(cudaMallocAsync(&d_out, sizeof(double), s));
-    int nb = std::min(mg->norm_blocks(), 4 * 148);
-    if (mg->kind == VDI_MG_FEM)
-        resid_norm_plain<double><<<nb, 256, 0, s>>>(mg->kind, CCc<double>{}, mg->femc<double>(0), z, b, r, mg->rd,
-                                                    d_out);
+    int nb = rblocks(mg->size(0));
+    if (mg->fem())
+        resid_out_k<double><<<nb, 256, 0, s>>>(mg->femc<double>(0), z, b, r, mg->rd, d_out);
     else
-        resid_norm_plain<double><<<nb, 256, 0, s>>>(mg->kind, mg->ccc<double>(0), FEMc<double>{}, z, b, r, mg->rd,
-                                                    d_out);
+        resid_out_k<double><<<nb, 256, 0, s>>>(mg->ccc<double>(0), z, b, r, mg->rd, d_out);
     VDI_CUDA(cudaGetLastError());
     double hn = 0;
     VDI_CUDA(cudaMemcpyAsync(&hn, d_out, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1137,10 +1249,10 @@ int mg_residual(MG* mg, cudaStream_t s, const double* b, const double* z, double
 
 int mg_apply(MG* mg, cudaStream_t s, const double* z, double* y) {
     long N = mg->size(0);
-    if (mg->kind == VDI_MG_FEM)
-        fem_apply<double><<<nblk(N), 256, 0, s>>>(mg->femc<double>(0), z, y);
+    if (mg->fem())
+        apply_k<double><<<nblk(N), 256, 0, s>>>(mg->femc<double>(0), z, y);
     else
-        cc_apply<double><<<nblk(N), 256, 0, s>>>(mg->ccc<double>(0), z, y);
+        apply_k<double><<<nblk(N), 256, 0, s>>>(mg->ccc<double>(0), z, y);
     VDI_CUDA(cudaGetLastError());
     return VDI_OK;
 }
