@@ -170,6 +170,21 @@ int vdi_mg_residual(vdi_mg* mg, const double* d_b, const double* d_z, double* d_
 /* y = A z, the operator of the problem class (a_cc*z + mul_a). */
 int vdi_mg_apply(vdi_mg* mg, const double* d_z, double* d_y);
 
+/* vdi_mg_solve_noalloc has no counterpart in the reference. It is the FP64
+ * solve of vdi_mg_create + vdi_mg_solve for callers that must not allocate
+ * device memory, such as an application that owns every device allocation
+ * itself or code running where an allocation would stall or fail. It
+ * allocates nothing: besides the caller's d_b and d_z it uses one static
+ * device array of about 5 MB that every GPU loading the library holds until
+ * exit. Grids are limited to 262144 unknowns (m*n); larger ones return
+ * VDI_ERR_UNSUPPORTED_SIZE. The first call on a device looks up the array's
+ * device address and should come before any stream capture. Calls share the
+ * array, so calls that overlap on the GPU (other streams or host threads)
+ * race. Arguments are those of vdi_mg_create and vdi_mg_solve; stream may
+ * be NULL. */
+int vdi_mg_solve_noalloc(int kind, int m, int n, double c1, double c2, int x_sym, const double* d_b, double* d_z,
+                         double rtol, int max_vcycles, void* stream, vdi_mg_result* res);
+
 /* ------------------------------------------------------- tridiagonal
  * tri_solve::solve_lapack (tri_solve.cc:24-33): solves the n x n system in
  * place (solution in d_d) on the GPU by cyclic reduction, falling back to

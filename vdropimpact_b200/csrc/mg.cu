@@ -1258,3 +1258,178 @@ int mg_apply(MG* mg, cudaStream_t s, const double* z, double* y) {
 }
 
 }  // namespace vdi
+
+// ======================================================= allocation-free solve
+// vdi_mg_solve_noalloc: the same FP64 multigrid solve as vdi_mg_create +
+// vdi_mg_solve, for callers that must not allocate device memory: an
+// application that owns every device allocation itself (a fixed memory
+// budget or its own pool), or code that runs where an allocation would
+// stall or fail (a real-time loop). Every device buffer the solve needs
+// beyond the caller's b and z comes from one file-scope __device__ array.
+
+namespace vdi {
+
+/** Largest problem the allocation-free solve accepts, in unknowns (cells for
+ * MAC and viscous systems, nodes for FEM). */
+static constexpr long NOALLOC_MAX_UNKNOWNS = 262144;
+/** Bytes of the static scratch array: the solve needs at most about
+ * 16 bytes per unknown for its scratch iterates and coarse levels, plus the
+ * reduction partials and control block. */
+static constexpr size_t NOALLOC_SCRATCH_BYTES = 16 * size_t(NOALLOC_MAX_UNKNOWNS) + (1u << 20);
+
+/** The scratch. It exists once on every device that loads the library and
+ * lives until the process exits. Calls share it: calls that overlap on the
+ * GPU (different streams, or different host threads) race on it. */
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+struct NoallocKey {
+    int dev, kind, m, n, x_sym;
+    double c1, c2;
+    bool operator==(const NoallocKey& o) const {
+        return dev == o.dev && kind == o.kind && m == o.m && n == o.n && x_sym == o.x_sym && c1 == o.c1 &&
+               c2 == o.c2;
+    }
+};
+
+struct NoallocEntry {
+    NoallocKey key;
+    MG* mg;
+};
+
+std::vector<NoallocEntry>& noalloc_cache() {
+    static std::vector<NoallocEntry> c;
+    return c;
+}
+
+/** Device address of g_noalloc_scratch on the current device, looked up once
+ * per device with that device current. */
+int noalloc_base(int dev, unsigned char** out) {
+    static std::vector<unsigned char*> base;
+    if (dev >= int(base.size())) base.resize(dev + 1, nullptr);
+    if (!base[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("vdi_mg_solve_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return VDI_ERR_CUDA;
+        }
+        base[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = base[dev];
+    return VDI_OK;
+}
+
+/** Builds an MG whose device buffers are carved from the static scratch. */
+int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
+    MG* g = new MG();
+    g->kind = k.kind; g->m = k.m; g->n = k.n; g->c1 = k.c1; g->c2 = k.c2; g->x_sym = k.x_sym;
+    int st = g->build_levels();
+    if (st != VDI_OK) {
+        delete g;
+        return st;
+    }
+    size_t off = 0;
+    bool fits = true;
+    auto take = [&](size_t bytes) -> unsigned char* {
+        off = (off + 255) & ~size_t(255);
+        unsigned char* p = base + off;
+        off += bytes;
+        if (off > NOALLOC_SCRATCH_BYTES) fits = false;
+        return p;
+    };
+    g->ctl = reinterpret_cast<SolveCtl*>(take(sizeof(SolveCtl)));
+    g->rd.counter = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
+    g->rd.partials = reinterpret_cast<double*>(take(sizeof(double) * MAX_PARTIALS));
+    g->rd.max_blocks = MAX_PARTIALS;
+    g->z64.assign(g->nlev, nullptr); g->b64.assign(g->nlev, nullptr); g->t64.assign(g->nlev, nullptr);
+    for (int l = 0; l < g->nlev; l++) {
+        size_t s = size_t(g->size(l)) * 8;
+        if (l < g->nmulti64) g->t64[l] = reinterpret_cast<double*>(take(s));
+        if (l > 0 && l <= g->nmulti64) {
+            g->z64[l] = reinterpret_cast<double*>(take(s));
+            g->b64[l] = reinterpret_cast<double*>(take(s));
+        }
+    }
+    auto forget = [&]() {
+        // the buffers belong to the static array: nothing to free
+        g->z64.clear(); g->b64.clear(); g->t64.clear();
+        g->ctl = nullptr;
+        g->rd.partials = nullptr;
+        g->rd.counter = nullptr;
+    };
+    if (!fits) {
+        set_error("vdi_mg_solve_noalloc: %dx%d needs %zu bytes of scratch, more than the %zu available", k.m, k.n,
+                  off, NOALLOC_SCRATCH_BYTES);
+        forget();
+        delete g;
+        return VDI_ERR_UNSUPPORTED_SIZE;
+    }
+    // shared-memory limits of the kernels this solve launches
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(cc_cta_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   int(CTA_SMEM_LIMIT));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fem_cta_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   int(CTA_SMEM_LIMIT));
+    if (e == cudaSuccess) e = tile_attr<double, 0, 0, CCc<double>>();
+    if (e == cudaSuccess) e = tile_attr<double, 0, 1, CCc<double>>();
+    if (e == cudaSuccess) e = tile_attr<double, 1, 0, FEMc<double>>();
+    if (e == cudaSuccess) e = tile_attr<double, 1, 1, FEMc<double>>();
+    if (e != cudaSuccess) {
+        set_error("vdi_mg_solve_noalloc: %s", cudaGetErrorString(e));
+        forget();
+        delete g;
+        return VDI_ERR_CUDA;
+    }
+    *out = g;
+    return VDI_OK;
+}
+
+}  // namespace
+}  // namespace vdi
+
+extern "C" int vdi_mg_solve_noalloc(int kind, int m, int n, double c1, double c2, int x_sym, const double* d_b,
+                                    double* d_z, double rtol, int max_vcycles, void* stream, vdi_mg_result* res) {
+    using namespace vdi;
+    if (!d_b || !d_z || !(rtol > 0) || max_vcycles < 0 || kind < 0 || kind > 3 || m < 2 || n < 2) {
+        set_error("vdi_mg_solve_noalloc: invalid arguments");
+        return VDI_ERR_INVALID_ARGUMENT;
+    }
+    if (long(m) * n > NOALLOC_MAX_UNKNOWNS) {
+        set_error("vdi_mg_solve_noalloc: %dx%d = %ld unknowns exceeds the maximum of %ld", m, n, long(m) * n,
+                  NOALLOC_MAX_UNKNOWNS);
+        return VDI_ERR_UNSUPPORTED_SIZE;
+    }
+    int dev = 0;
+    VDI_CUDA(cudaGetDevice(&dev));
+    unsigned char* base = nullptr;
+    VDI_TRY(noalloc_base(dev, &base));
+    NoallocKey key{dev, kind, m, n, x_sym, c1, c2};
+    if (kind == VDI_MG_MAC) {
+        // mgs_mac.cc:23-27 (test constructor): xxsp = 1/(dx*dx)
+        key.c1 = 1. / (c1 * c1);
+        key.c2 = 1. / (c2 * c2);
+    }
+    MG* g = nullptr;
+    for (auto& e : noalloc_cache())
+        if (e.key == key) g = e.mg;
+    if (!g) {
+        VDI_TRY(noalloc_build(key, base, &g));
+        noalloc_cache().push_back(NoallocEntry{key, g});
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the array keeps the previous call's contents: restart the control
+    // block and the reduction counter
+    VDI_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SolveCtl), s));
+    VDI_CUDA(cudaMemsetAsync(g->rd.counter, 0, sizeof(unsigned), s));
+    VDI_TRY(g->set_ctl_params(s, rtol, max_vcycles));
+    int v = 0;
+    double r = 0;
+    int st = mg_solve(g, s, d_b, d_z, rtol, max_vcycles, VDI_MG_FP64, &v, &r);
+    if (res) {
+        res->vcycles = v;
+        res->rel_res = r;
+    }
+    return st;
+}
