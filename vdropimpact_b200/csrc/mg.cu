@@ -27,6 +27,7 @@
 #include "vdi_internal.hh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 
@@ -445,6 +446,152 @@ __global__ void __launch_bounds__(TileDims<T, KIND, SMALL>::NT) mg_tile(OP c, Ti
     }
 }
 
+// ------------------------------------------ red-black split cell-centred tile
+// The 5-point systems use their own tile kernel: a 64 x 64 window stored as
+// two colour arrays, S_c[jj][k] = window point (2k + p, jj) of colour c, so a
+// warp updates one colour-row with 32 consecutive shared-memory words and its
+// four neighbours are also consecutive words. Every colour phase updates the
+// whole window; points within K rings of the window edge go stale one ring per
+// phase, which the halo of ZH = K + 1 rings keeps out of the interior results.
+// Tiles away from the grid edge skip all boundary tests.
+template <typename T, int NS>
+struct CCTile {
+    static constexpr int CW = 64, CH = 64, KW = CW / 2;
+    static constexpr int K = 2 * NS, ZH = K + 1;
+    static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
+    static constexpr int NT = 512, NW = NT / 32;
+    static constexpr size_t smem = size_t(4) * CH * KW * sizeof(T);
+};
+
+/** MODE 0: NS sweeps from zin (or zero), residual, restriction to bc (skipped
+ * when bc is null). MODE 1: zin + prolonged zc, NS sweeps, and optionally the
+ * residual norm with the solve decision. Both write zout. */
+template <typename T, int MODE, int NS>
+__global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<T> a) {
+    using G = CCTile<T, NS>;
+    constexpr int CW = G::CW, CH = G::CH, KW = G::KW, ZH = G::ZH, TX = G::TX, TY = G::TY, K = G::K;
+    constexpr int NW = G::NW, RPW = CH / NW;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* Z = reinterpret_cast<T*>(sm_raw);
+    T* B = Z + 2 * CH * KW;
+    const int m = c.m, n = c.n;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zx = x0 - ZH, zy = y0 - ZH;
+    const int par0 = (zx + zy) & 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool inner = zx >= 0 && zy >= 0 && zx + CW <= m && zy + CH <= n;
+    const bool read_z = MODE == 1 || !a.zero_init;
+    // ---- load: every load of the thread issued before the shared stores
+    {
+        T zv[RPW][2], bv[RPW][2];
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            int jj = warp + q * NW, j = zy + jj;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int i = zx + lane + 32 * h;
+                bool in = unsigned(i) < unsigned(m) && unsigned(j) < unsigned(n);
+                zv[q][h] = (in && read_z) ? a.zin[i + m * j] : T(0);
+                bv[q][h] = in ? a.b[i + m * j] : T(0);
+                if (MODE == 1 && in) zv[q][h] += cc_interp(c, a.zc, i, j);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            int jj = warp + q * NW;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int ii = lane + 32 * h;
+                int col = (par0 + ii + jj) & 1;
+                Z[col * CH * KW + jj * KW + (ii >> 1)] = zv[q][h];
+                B[col * CH * KW + jj * KW + (ii >> 1)] = bv[q][h];
+            }
+        }
+    }
+    __syncthreads();
+    // ---- colour phases
+#pragma unroll
+    for (int ph = 0; ph < K; ph++) {
+        const int color = MODE == 1 ? ((ph & 1) ^ 1) : (ph & 1);
+        T* Zc = Z + color * CH * KW;
+        const T* Zo = Z + (color ^ 1) * CH * KW;
+        const T* Bc = B + color * CH * KW;
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            const int jj = warp + q * NW;
+            if (jj < 1 || jj > CH - 2) continue;
+            const int p = (color ^ par0 ^ jj) & 1;
+            const int ii = 2 * lane + p;
+            if (ii == 0 || ii == CW - 1) continue;
+            const T* zo = Zo + jj * KW;
+            const T l = zo[lane - 1 + p], r = zo[lane + p];
+            const T d = Zo[(jj - 1) * KW + lane], u = Zo[(jj + 1) * KW + lane];
+            T* w = Zc + jj * KW + lane;
+            if (inner) {
+                *w = (Bc[jj * KW + lane] - (c.ox * (l + r) + c.oy * (d + u))) * c.invd[1][1];
+            } else {
+                const int i = zx + ii, j = zy + jj;
+                if (unsigned(i) >= unsigned(m) || unsigned(j) >= unsigned(n)) continue;
+                T xs = (i > 0 ? l : T(0)) + (i < m - 1 ? r : T(0));
+                T ys = (j > 0 ? d : T(0)) + (j < n - 1 ? u : T(0));
+                *w = (Bc[jj * KW + lane] - (c.ox * xs + c.oy * ys)) * c.invd[cls(i, m)][cls(j, n)];
+            }
+        }
+        __syncthreads();
+    }
+    // ---- epilogue helpers over window coordinates
+    auto zat = [&](int ii, int jj) -> T { return Z[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)]; };
+    auto resid = [&](int ii, int jj) -> T {
+        const int i = zx + ii, j = zy + jj;
+        T bv = B[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)];
+        T xs = (i > 0 ? zat(ii - 1, jj) : T(0)) + (i < m - 1 ? zat(ii + 1, jj) : T(0));
+        T ys = (j > 0 ? zat(ii, jj - 1) : T(0)) + (j < n - 1 ? zat(ii, jj + 1) : T(0));
+        return bv - c.d[cls(i, m)][cls(j, n)] * zat(ii, jj) - (c.ox * xs + c.oy * ys);
+    };
+    // interior back to global memory (coalesced by row)
+    for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
+        const int j = zy + jj;
+        if (j >= n) break;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int ii = ZH + lane + 32 * h;
+            const int i = zx + ii;
+            if (ii < ZH + TX && i < m) a.zout[i + m * j] = zat(ii, jj);
+        }
+    }
+    if (MODE == 0) {
+        if (a.bc) {
+            const int mc = m >> 1, nc = n >> 1;
+            constexpr int CX = TX / 2, CY = TY / 2;
+            for (int t = threadIdx.x; t < CX * CY; t += G::NT) {
+                const int q = t / CX;
+                const int I = x0 / 2 + (t - q * CX), J = y0 / 2 + q;
+                if (I >= mc || J >= nc) continue;
+                const int ii = 2 * I - zx, jj = 2 * J - zy;
+                T s = resid(ii, jj) + resid(ii + 1, jj) + resid(ii, jj + 1) + resid(ii + 1, jj + 1);
+                a.bc[I + mc * J] = T(0.25) * s;
+            }
+        }
+    } else if (a.norm) {
+        double s = 0;
+        for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
+            const int j = zy + jj;
+            if (j >= n) break;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int ii = ZH + lane + 32 * h;
+                if (ii < ZH + TX && zx + ii < m) {
+                    double r = double(resid(ii, jj));
+                    s += r * r;
+                }
+            }
+        }
+        s = block_sum(s);
+        double total;
+        if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
+    }
+}
+
 // ---------------------------------------------------- CTA-resident levels
 template <typename T>
 struct CCStack {
@@ -462,29 +609,32 @@ struct FEMStack {
     int nu1, nu2, ncoarse;
 };
 
-/** One colour of a whole-level sweep inside the CTA (colour-indexed). */
+/** Row loops of the CTA-resident levels: warp w takes rows w, w+nw, ...;
+ * lanes take columns, so no index division is needed. */
+#define CTA_ROWS(j, j0, jstep, nrows) \
+    for (int j = (j0) + (threadIdx.x >> 5) * (jstep); j < (nrows); j += (blockDim.x >> 5) * (jstep))
+
+/** One colour of a whole-level sweep inside the CTA. */
 template <typename T>
 __device__ void cta_sweep(const CCc<T>& c, T* z, const T* b, int color) {
-    const int half = (c.m + 1) >> 1, tot = half * c.n;
-    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-        int j = t / half;
-        int i = 2 * (t - j * half) + ((color ^ j) & 1);
-        if (i >= c.m) continue;
-        T* w = z + i + c.m * j;
-        *w = op_relaxed(c, w, b[i + c.m * j], c.m, i, j);
+    const int lane = threadIdx.x & 31;
+    CTA_ROWS(j, 0, 1, c.n) {
+        for (int i = 2 * lane + ((color ^ j) & 1); i < c.m; i += 64) {
+            T* w = z + i + c.m * j;
+            *w = op_relaxed(c, w, b[i + c.m * j], c.m, i, j);
+        }
     }
     __syncthreads();
 }
 
 template <typename T>
 __device__ void cta_sweep(const FEMc<T>& c, T* z, const T* b, int color) {
-    const int ci = color & 1, cj = color >> 1;
-    const int W2 = (c.M - ci + 1) >> 1, H2 = (c.N - cj + 1) >> 1, tot = W2 * H2;
-    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-        int q = t / W2;
-        int i = ci + 2 * (t - q * W2), j = cj + 2 * q;
-        T* w = z + i + c.M * j;
-        *w = op_relaxed(c, w, b[i + c.M * j], c.M, i, j);
+    const int ci = color & 1, cj = color >> 1, lane = threadIdx.x & 31;
+    CTA_ROWS(j, cj, 2, c.N) {
+        for (int i = ci + 2 * lane; i < c.M; i += 64) {
+            T* w = z + i + c.M * j;
+            *w = op_relaxed(c, w, b[i + c.M * j], c.M, i, j);
+        }
     }
     __syncthreads();
 }
@@ -494,11 +644,13 @@ __global__ void __launch_bounds__(CTA_THREADS) cc_cta_cycle(CCStack<T> st, const
                                                            T* __restrict__ gz, int zero_init) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
+    const int lane = threadIdx.x & 31;
     {
         const CCc<T>& c0 = st.lv[0];
         T* z = sm + st.off[0];
         T* b = z + c0.m * c0.n;
-        for (int k = threadIdx.x; k < c0.m * c0.n; k += blockDim.x) {
+        const int tot = c0.m * c0.n;
+        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
             b[k] = gb[k];
             z[k] = zero_init ? T(0) : gz[k];
         }
@@ -518,15 +670,16 @@ __global__ void __launch_bounds__(CTA_THREADS) cc_cta_cycle(CCStack<T> st, const
         }
         const CCc<T>& cc = st.lv[l + 1];
         T* bcn = sm + st.off[l + 1] + cc.m * cc.n;
-        for (int k = threadIdx.x; k < cc.m * cc.n; k += blockDim.x) {
-            int J = k / cc.m, I = k - J * cc.m;
-            T s = 0;
-            for (int dj = 0; dj < 2; dj++)
-                for (int di = 0; di < 2; di++) {
-                    int i = 2 * I + di, j = 2 * J + dj;
-                    s += op_resid(c, z + i + c.m * j, b[i + c.m * j], c.m, i, j);
-                }
-            bcn[k] = T(0.25) * s;
+        CTA_ROWS(J, 0, 1, cc.n) {
+            for (int I = lane; I < cc.m; I += 32) {
+                T s = 0;
+                for (int dj = 0; dj < 2; dj++)
+                    for (int di = 0; di < 2; di++) {
+                        int i = 2 * I + di, j = 2 * J + dj;
+                        s += op_resid(c, z + i + c.m * j, b[i + c.m * j], c.m, i, j);
+                    }
+                bcn[I + cc.m * J] = T(0.25) * s;
+            }
         }
         __syncthreads();
     }
@@ -545,9 +698,8 @@ __global__ void __launch_bounds__(CTA_THREADS) cc_cta_cycle(CCStack<T> st, const
         T* z = sm + st.off[l];
         T* b = z + c.m * c.n;
         const T* zc = sm + st.off[l + 1];
-        for (int k = threadIdx.x; k < c.m * c.n; k += blockDim.x) {
-            int j = k / c.m, i = k - j * c.m;
-            z[k] += cc_interp(c, zc, i, j);
+        CTA_ROWS(j, 0, 1, c.n) {
+            for (int i = lane; i < c.m; i += 32) z[i + c.m * j] += cc_interp(c, zc, i, j);
         }
         __syncthreads();
         for (int s = 0; s < st.nu2; s++) {
@@ -567,6 +719,7 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
                                                             T* __restrict__ gz, int zero_init) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
+    const int lane = threadIdx.x & 31;
     {
         const FEMc<T>& c0 = st.lv[0];
         T* z = sm + st.off[0];
@@ -583,22 +736,23 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
     __syncthreads();
     for (int l = 0; l < st.nl - 1; l++) {
         const FEMc<T>& c = st.lv[l];
-        int tot = c.M * c.N;
+        const int tot = c.M * c.N;
         T* z = sm + st.off[l];
         T* b = z + tot;
         T* r = b + tot;
         for (int s = 0; s < st.nu1; s++)
             for (int q = 0; q < 4; q++) cta_sweep(c, z, b, q);
-        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
-            int j = k / c.M, i = k - j * c.M;
-            r[k] = op_resid(c, z + k, b[k], c.M, i, j);
+        CTA_ROWS(j, 0, 1, c.N) {
+            for (int i = lane; i < c.M; i += 32) {
+                int k = i + c.M * j;
+                r[k] = op_resid(c, z + k, b[k], c.M, i, j);
+            }
         }
         __syncthreads();
         const FEMc<T>& cc = st.lv[l + 1];
         T* bcn = sm + st.off[l + 1] + cc.M * cc.N;
-        for (int k = threadIdx.x; k < cc.M * cc.N; k += blockDim.x) {
-            int J = k / cc.M, I = k - J * cc.M;
-            bcn[k] = fem_restrict_at(c.M, c.N, r, c.M, 0, 0, I, J);
+        CTA_ROWS(J, 0, 1, cc.N) {
+            for (int I = lane; I < cc.M; I += 32) bcn[I + cc.M * J] = fem_restrict_at(c.M, c.N, r, c.M, 0, 0, I, J);
         }
         __syncthreads();
     }
@@ -612,13 +766,12 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
     }
     for (int l = st.nl - 2; l >= 0; l--) {
         const FEMc<T>& c = st.lv[l];
-        int tot = c.M * c.N;
+        const int tot = c.M * c.N;
         T* z = sm + st.off[l];
         T* b = z + tot;
         const T* zc = sm + st.off[l + 1];
-        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
-            int j = k / c.M, i = k - j * c.M;
-            z[k] += fem_interp(c, zc, i, j);
+        CTA_ROWS(j, 0, 1, c.N) {
+            for (int i = lane; i < c.M; i += 32) z[i + c.M * j] += fem_interp(c, zc, i, j);
         }
         __syncthreads();
         for (int s = 0; s < st.nu2; s++)
@@ -764,6 +917,21 @@ static cudaError_t tile_attr() {
                                 int(tile_smem<T, KIND, MODE, 2, 1>()));
 }
 
+template <typename T, int MODE>
+static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T>& a) {
+    using G = CCTile<T, 2>;
+    dim3 grid((c.m + G::TX - 1) / G::TX, (c.n + G::TY - 1) / G::TY);
+    cc_tile<T, MODE, 2><<<grid, G::NT, G::smem, s>>>(c, a);
+}
+
+template <typename T>
+static cudaError_t cc_tile_attr() {
+    using G = CCTile<T, 2>;
+    cudaError_t e = cudaFuncSetAttribute(cc_tile<T, 0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(cc_tile<T, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+}
+
 class MG {
   public:
     int kind = 0;
@@ -774,6 +942,8 @@ class MG {
     FEMOp fop{};
     int nlev = 0;
     int nmulti64 = 0, nmulti32 = 0;
+    // the coarsest level is solved by tile smoothing instead of the CTA cycle
+    bool smooth_tail = false;
     size_t smem64 = 0, smem32 = 0;
     // device buffers: index l holds level l (level 0 of z64/b64 is the caller's)
     std::vector<double*> z64, b64, t64;
@@ -901,11 +1071,25 @@ class MG {
                 fill_cc(L, kx, ky);
                 lv.push_back(L);
                 if ((mm & 1) || (nn & 1) || mm < 4 || nn < 2 || int(lv.size()) == MAXLEV) break;
+                // The viscous operator I - vfx Dxx - vfy Dyy is close to the
+                // identity once 2(vfx+vfy) is small: Gauss-Seidel alone solves
+                // that level, and coarser levels add nothing.
+                if (kind != VDI_MG_MAC && lv.size() >= 2 && 2 * (kx + ky) < 0.25) break;
                 mm >>= 1; nn >>= 1;
                 kx *= 0.25; ky *= 0.25;
             }
         }
         nlev = int(lv.size());
+        smooth_tail = kind == VDI_MG_VISC_U || kind == VDI_MG_VISC_V;
+        if (smooth_tail) {
+            if (nlev < 2) {
+                set_error("multigrid: viscous %dx%d grid cannot coarsen", m, n);
+                return VDI_ERR_UNSUPPORTED_SIZE;
+            }
+            nmulti64 = nmulti32 = nlev - 1;
+            smem64 = smem32 = 0;
+            return VDI_OK;
+        }
         // the CTA-resident tail must fit in shared memory
         int arrays = fem() ? 3 : 2;
         auto tail_bytes = [&](int from, size_t es) {
@@ -965,6 +1149,8 @@ class MG {
         VDI_CUDA((tile_attr<double, 1, 1, FEMc<double>>()));
         VDI_CUDA((tile_attr<float, 1, 0, FEMc<float>>()));
         VDI_CUDA((tile_attr<float, 1, 1, FEMc<float>>()));
+        VDI_CUDA(cc_tile_attr<double>());
+        VDI_CUDA(cc_tile_attr<float>());
         return VDI_OK;
     }
 
@@ -995,6 +1181,13 @@ class MG {
     template <typename T>
     int vcycle(cudaStream_t s, int l, const T* b, T* z, int nmulti, std::vector<T*>& zs, std::vector<T*>& bs,
                size_t smem, int zero_init, int norm, int use_cond, cudaGraphConditionalHandle h) {
+        if (l == nmulti && smooth_tail) {
+            TileArgs<T> a = targs<T>(nullptr, z, b);
+            a.zero_init = 1;
+            launch_cc_tile<T, 0>(s, ccc<T>(l), a);
+            VDI_CUDA(cudaGetLastError());
+            return VDI_OK;
+        }
         if (l == nmulti) {
             if (fem()) {
                 FEMStack<T> st{};
@@ -1028,7 +1221,7 @@ class MG {
         a.zero_init = zero_init;
         a.bc = bs[l + 1];
         if (fem()) launch_tile<T, 1, 0>(s, femc<T>(l), a, lv[l].m, lv[l].n);
-        else launch_tile<T, 0, 0>(s, ccc<T>(l), a, lv[l].m, lv[l].n);
+        else launch_cc_tile<T, 0>(s, ccc<T>(l), a);
         VDI_CUDA(cudaGetLastError());
         VDI_TRY(vcycle<T>(s, l + 1, bs[l + 1], zs[l + 1], nmulti, zs, bs, smem, 1, 0, 0, 0));
         TileArgs<T> p = targs<T>(zs_tmp, z, b);
@@ -1037,7 +1230,7 @@ class MG {
         p.use_cond = use_cond;
         p.h = h;
         if (fem()) launch_tile<T, 1, 1>(s, femc<T>(l), p, lv[l].m, lv[l].n);
-        else launch_tile<T, 0, 1>(s, ccc<T>(l), p, lv[l].m, lv[l].n);
+        else launch_cc_tile<T, 1>(s, ccc<T>(l), p);
         VDI_CUDA(cudaGetLastError());
         return VDI_OK;
     }
@@ -1140,14 +1333,17 @@ void mg_destroy(MG* mg) { delete mg; }
 
 int mg_set_visc(MG* mg, double vfx, double vfy) {
     if (mg->kind != VDI_MG_VISC_U && mg->kind != VDI_MG_VISC_V) return VDI_ERR_INVALID_ARGUMENT;
+    // the hierarchy depth depends on vfx, vfy: rebuild it (visco_impl::setup,
+    // called by setup_and_solve when vfx changes, visco_impl.cc:26-30)
+    double rt = mg->rtol;
+    int mx = mg->max_it;
+    mg->release();
     mg->c1 = vfx;
     mg->c2 = vfy;
-    double kx = vfx, ky = vfy;
-    for (auto& L : mg->lv) {
-        mg->fill_cc(L, kx, ky);
-        kx *= 0.25; ky *= 0.25;
-    }
-    return VDI_OK;
+    mg->rtol = rt;
+    mg->max_it = mx;
+    VDI_TRY(mg->build_levels());
+    return mg->alloc();
 }
 
 SolveCtl* mg_ctl(MG* mg) { return mg->ctl; }
@@ -1376,6 +1572,7 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
     if (e == cudaSuccess) e = tile_attr<double, 0, 1, CCc<double>>();
     if (e == cudaSuccess) e = tile_attr<double, 1, 0, FEMc<double>>();
     if (e == cudaSuccess) e = tile_attr<double, 1, 1, FEMc<double>>();
+    if (e == cudaSuccess) e = cc_tile_attr<double>();
     if (e != cudaSuccess) {
         set_error("vdi_mg_solve_noalloc: %s", cudaGetErrorString(e));
         forget();
