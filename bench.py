@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only", default="", help="run only 'plain' or 'fast' (profiling)")
     ap.add_argument("--eager", action="store_true", help="launch kernels without CUDA graphs (profiling)")
+    ap.add_argument("--fast-precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--fast-guess", default="quadratic", choices=["linear", "quadratic", "learned"])
     return ap.parse_args()
 
 
@@ -189,8 +191,9 @@ def run_reference_arm(args, ws, rank):
 
 
 # ----------------------------------------------------------------- ours
-def time_config(V, torch, text, args, precision, stream, ws, clocks=None):
-    f = V.Fluid2D(text, mg_rtol=args.rtol, mg_precision=precision, graph=not args.eager, stream=stream)
+def time_config(V, torch, text, args, precision, guess, stream, ws, clocks=None):
+    f = V.Fluid2D(text, mg_rtol=args.rtol, mg_precision=precision, mg_guess=guess, graph=not args.eager,
+                  stream=stream)
     f.init_fields()
     dt = f.frame_dt()
     f.step_forward(dt, args.warmup)
@@ -213,6 +216,37 @@ def time_config(V, torch, text, args, precision, stream, ws, clocks=None):
     solves = sum(st["solves"].values())
     vc = {k: st["vcycles"][k] / max(st["solves"][k], 1) for k in st["vcycles"]}
     return f, dt, ms, vc, st, ck, solves
+
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# DRAM bytes (read + write) of one launch of the roofline kernel in an ncu
+# capture; see profiles/cc_tile_post_fp64_2048x1024.md.
+CC_POST_DRAM_BYTES = None
+
+
+def roofline(V, torch, args):
+    """The dominant kernel of the step: the finest-level post-smoothing tile
+    kernel of the cell-centred solves (MAC and both viscous systems), timed
+    with CUDA events on its own stream over repeated launches at the bench
+    grid. Algorithmic bytes per launch: z in, b in, z out (8 B each per cell)
+    plus the coarse correction (8 B per coarse cell)."""
+    m, n = (int(x) for x in args.grid.split("x"))
+    s = V.MgsMac(m, n, 1.0 / m, 1.0 / m)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    s.b.copy_(torch.randn(m * n, dtype=torch.float64, device="cuda", generator=g))
+    ms, nbytes = s.profile(1, 100)
+    peak, kind = measured_peak_gbs()
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"kernel": "cc_tile<double, POST> on the 2048x1024 MAC grid", "bound": "hbm", "achieved": achieved,
+            "peak": peak, "peak_source": kind, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": CC_POST_DRAM_BYTES, "algorithmic_bytes": nbytes, "ms_per_launch": ms}
 
 
 def e2e_run(V, torch, f, dt, stream, steps, ws):
@@ -268,14 +302,15 @@ def main():
     text = cfg_text(args.grid)
     stream = torch.cuda.Stream()
     results = {}
-    modes = [("plain", "fp64"), ("fast", "mixed")]
+    modes = [("plain", "fp64", "linear"), ("fast", args.fast_precision, args.fast_guess)]
     if args.only:
         modes = [m for m in modes if m[0] == args.only]
     keep = None
-    for name, prec in modes:
+    for name, prec, guess in modes:
         clocks = ClockSampler(local) if name == "fast" or args.only else None
-        f, dt, ms, vc, st, ck, solves = time_config(V, torch, text, args, prec, stream, ws, clocks)
-        results[name] = dict(ms=ms, vc=vc, clocks=ck, solves=solves, newton=st["newton_steps"])
+        f, dt, ms, vc, st, ck, solves = time_config(V, torch, text, args, prec, guess, stream, ws, clocks)
+        results[name] = dict(ms=ms, vc=vc, clocks=ck, solves=solves, newton=st["newton_steps"],
+                             launches=st["kernel_launches"])
         if name == modes[-1][0]:
             keep = (f, dt)
         else:
@@ -293,7 +328,7 @@ def main():
                    "parallelism": f"replicas x{ws}"},
         "clocks": head["clocks"],
         "vcycles_per_solve": head["vc"],
-        "gpu_launches": None,
+        "gpu_launches": head["launches"],
     }
     if "plain" in results:
         p = results["plain"]
@@ -301,6 +336,7 @@ def main():
                               "vcycles_per_solve": p["vc"]}
         line["speedup_vs_plain_fp64"] = p["ms"] / head["ms"]
     f, dt = keep
+    line["roofline"] = roofline(V, torch, args)
     if not args.no_e2e:
         e2e_steps = max(3, min(args.steps, 50))
         ms, bi, bo = e2e_run(V, torch, f, dt, stream, e2e_steps, ws)

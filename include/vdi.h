@@ -78,7 +78,9 @@ enum vdi_mg_precision {
 };
 enum vdi_mg_guess {
     VDI_GUESS_EXTRAPOLATE = 0, /* linear time extrapolation (mgs_common.cc:17-50) */
-    VDI_GUESS_LEARNED = 1      /* U-Net prediction added to the extrapolation */
+    VDI_GUESS_LEARNED = 1,     /* U-Net prediction added to the extrapolation */
+    VDI_GUESS_QUADRATIC = 2    /* quadratic extrapolation in time from the last
+                                  three solutions (starting iterate only) */
 };
 
 /* Parses a vdropimpact .cfg text (fileinfo.cc:11-193; gas_layer_model only)
@@ -132,6 +134,7 @@ typedef struct vdi_stats {
     long tri_pivot_fallbacks; /* tridiagonal solves that needed pivoting */
     long height_fixed_point_iters;
     double last_rel_res[4];
+    long kernel_launches;     /* kernels this library launched for the counted steps */
 } vdi_stats;
 int vdi_sim_stats(vdi_sim* sim, vdi_stats* out, int reset);
 
@@ -169,6 +172,14 @@ int vdi_mg_v_cycle(vdi_mg* mg, const double* d_b, double* d_z);
 int vdi_mg_residual(vdi_mg* mg, const double* d_b, const double* d_z, double* d_r, double* norm);
 /* y = A z, the operator of the problem class (a_cc*z + mul_a). */
 int vdi_mg_apply(vdi_mg* mg, const double* d_z, double* d_y);
+/* Measurement helper: launches the finest-level smoothing kernel of one
+ * V-cycle (which = 0 the pre-smoothing/restriction kernel, 1 the
+ * prolongation/post-smoothing kernel) iters times on d_b, d_z between two
+ * CUDA events on the system's stream, and returns the mean duration per
+ * launch and the kernel's algorithmic bytes per launch (each input and output
+ * array read or written once). */
+int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
+                   double* bytes_per_launch);
 
 /* vdi_mg_solve_noalloc has no counterpart in the reference. It is the FP64
  * solve of vdi_mg_create + vdi_mg_solve for callers that must not allocate

@@ -54,10 +54,13 @@ def params_from_cfg(cfg: str) -> _abi.VdiParams:
 class Fluid2D:
     """fluid_2d (fluid_2d.hh:21-142) on the GPU."""
 
+    GUESS = {"linear": 0, "learned": 1, "quadratic": 2}
+
     def __init__(self, cfg, *, mg_rtol: float = 1e-10, mg_max_vcycles: int = 200,
-                 mg_precision="fp64", graph: bool = False, stream=None):
+                 mg_precision="fp64", mg_guess="linear", graph: bool = False, stream=None):
         self.prm = cfg if isinstance(cfg, _abi.VdiParams) else params_from_cfg(cfg)
         self.prm.mg_rtol = mg_rtol
+        self.prm.mg_guess = self.GUESS[mg_guess] if isinstance(mg_guess, str) else int(mg_guess)
         self.prm.mg_max_vcycles = mg_max_vcycles
         self.prm.mg_precision = _PREC[mg_precision]
         self.m, self.n = self.prm.m, self.prm.n
@@ -170,7 +173,7 @@ class Fluid2D:
                     vcycles=dict(zip(names, list(s.vcycles))), newton_steps=s.newton_steps,
                     tri_pivot_fallbacks=s.tri_pivot_fallbacks,
                     height_fixed_point_iters=s.height_fixed_point_iters,
-                    last_rel_res=dict(zip(names, list(s.last_rel_res))))
+                    last_rel_res=dict(zip(names, list(s.last_rel_res))), kernel_launches=s.kernel_launches)
 
     def device_field(self, which: int):
         p = _abi._dp()
@@ -235,6 +238,16 @@ class _MgSystem:
         torch.cuda.synchronize()
         check(lib().vdi_mg_apply(self._h, C.c_void_p(z.data_ptr()), C.c_void_p(y.data_ptr())), "vdi_mg_apply")
         return y
+
+    def profile(self, which: int = 1, iters: int = 50):
+        """Mean duration (ms) and algorithmic bytes of one launch of the
+        finest-level pre- (0) or post- (1) smoothing kernel."""
+        ms = C.c_float()
+        by = C.c_double()
+        _torch().cuda.synchronize()
+        check(lib().vdi_mg_profile(self._h, which, iters, C.c_void_p(self.b.data_ptr()),
+                                   C.c_void_p(self.z.data_ptr()), C.byref(ms), C.byref(by)), "vdi_mg_profile")
+        return ms.value, by.value
 
     def residual(self):
         """(r, ||r||_2) with r = b - A z (tgmg::output_res)."""

@@ -28,6 +28,7 @@ VDI_MG_FP64 = 0
 VDI_MG_MIXED = 1
 VDI_GUESS_EXTRAPOLATE = 0
 VDI_GUESS_LEARNED = 1
+VDI_GUESS_QUADRATIC = 2
 
 VDI_MG_MAC = 0
 VDI_MG_FEM = 1
@@ -58,7 +59,8 @@ class VdiState(C.Structure):
 class VdiStats(C.Structure):
     _fields_ = [("steps", C.c_long), ("solves", C.c_long * 4), ("vcycles", C.c_long * 4),
                 ("newton_steps", C.c_long), ("tri_pivot_fallbacks", C.c_long),
-                ("height_fixed_point_iters", C.c_long), ("last_rel_res", C.c_double * 4)]
+                ("height_fixed_point_iters", C.c_long), ("last_rel_res", C.c_double * 4),
+                ("kernel_launches", C.c_long)]
 
 
 class VdiMgResult(C.Structure):
@@ -107,6 +109,8 @@ _SIGS = [
     ("vdi_mg_v_cycle", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("vdi_mg_residual", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     ("vdi_mg_apply", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("vdi_mg_profile", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_float),
+                                 _dp]),
     ("vdi_tri_solve", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.POINTER(C.c_int)]),
 ]

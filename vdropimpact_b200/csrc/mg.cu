@@ -592,6 +592,168 @@ __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<
     }
 }
 
+// -------------------------------------- four-colour split node-centred tile
+// The FEM system's tile: a 64 x 64 window with an even origin, so window point
+// (ii,jj) has colour (ii&1, jj&1); each colour lives in its own 32 x 32
+// quarter array Q[ci+2cj][jj>>1][ii>>1]. A warp updates one quarter-row with
+// 32 consecutive words; all eight neighbours are consecutive words of the
+// other quarters. As in the cell-centred tile, every phase updates the whole
+// window and the halo (10 rings for 8 colour phases plus the residual ring of
+// the restriction) keeps the stale edge out of the interior results.
+template <typename T>
+struct FEMTile {
+    static constexpr int CW = 64, CH = 64, QW = 32, QN = QW * QW;
+    static constexpr int K = 8, ZH = 10;
+    static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
+    static constexpr int RW = TX + 2, RH = TY + 2;
+    static constexpr int NT = 512, NW = NT / 32;
+    static constexpr size_t smem = (size_t(8) * QN + size_t(RW) * RH) * sizeof(T);
+};
+
+/** mul_a of mgs_fem.cc:32-53 from neighbour values (dl d dr / l r / ul u ur). */
+template <typename T>
+__device__ __forceinline__ T fem_off_vals(const FEMc<T>& c, int i, int j, T dl, T d, T dr, T l, T r, T ul, T u,
+                                          T ur) {
+    if (j == 0) return T(0);
+    if (j == c.N - 1) {
+        if (i == 0) return c.fc * dr + c.hey * d + c.hex * r;
+        if (i == c.M - 1) return c.fc * dl + c.hey * d + c.hex * l;
+        return c.fc * (dl + dr) + c.fey * d + c.hex * (l + r);
+    }
+    if (i == 0) return c.fc * (dr + ur) + c.hey * (d + u) + c.fex * r;
+    if (i == c.M - 1) return c.fc * (dl + ul) + c.hey * (d + u) + c.fex * l;
+    return c.fc * (dl + dr + ul + ur) + c.fey * (d + u) + c.fex * (l + r);
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T> a) {
+    using G = FEMTile<T>;
+    constexpr int QW = G::QW, QN = G::QN, ZH = G::ZH, TX = G::TX, TY = G::TY, K = G::K, NW = G::NW;
+    constexpr int CH = G::CH, RW = G::RW, RH = G::RH;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* Z = reinterpret_cast<T*>(sm_raw);     // 4 quarters
+    T* B = Z + 4 * QN;                       // 4 quarters
+    T* R = B + 4 * QN;                       // residual ring array (PRE)
+    const int M = c.M, N = c.N;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zx = x0 - ZH, zy = y0 - ZH;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool inner = zx >= 0 && zy >= 0 && zx + G::CW <= M && zy + CH <= N && zy > 0;
+    const bool read_z = MODE == 1 || !a.zero_init;
+    auto qidx = [](int ii, int jj) { return ((ii & 1) + 2 * (jj & 1)) * QN + (jj >> 1) * QW + (ii >> 1); };
+    {
+        constexpr int RPW = CH / NW;
+        T zv[RPW][2], bv[RPW][2];
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            int jj = warp + q * NW, j = zy + jj;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int i = zx + lane + 32 * h;
+                bool in = unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N);
+                zv[q][h] = (in && read_z) ? a.zin[i + M * j] : T(0);
+                bv[q][h] = in ? a.b[i + M * j] : T(0);
+                if (MODE == 1 && in) zv[q][h] += fem_interp(c, a.zc, i, j);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            int jj = warp + q * NW;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int ii = lane + 32 * h;
+                Z[qidx(ii, jj)] = zv[q][h];
+                B[qidx(ii, jj)] = bv[q][h];
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ph = 0; ph < K; ph++) {
+        const int color = MODE == 1 ? 3 - (ph & 3) : (ph & 3);
+        const int ci = color & 1, cj = color >> 1;
+        T* Zc = Z + color * QN;
+        const T* Zx = Z + (color ^ 1) * QN;   // (1-ci, cj): left/right
+        const T* Zy = Z + (color ^ 2) * QN;   // (ci, 1-cj): down/up
+        const T* Zd = Z + (color ^ 3) * QN;   // (1-ci, 1-cj): diagonals
+        const T* Bc = B + color * QN;
+#pragma unroll
+        for (int q = 0; q < QW / NW; q++) {
+            const int jr = warp + q * NW, ir = lane;
+            const int ii = 2 * ir + ci, jj = 2 * jr + cj;
+            if (ii == 0 || ii == G::CW - 1 || jj == 0 || jj == CH - 1) continue;
+            const int xl = ir - 1 + ci, xr = ir + ci, yd = jr - 1 + cj, yu = jr + cj;
+            const T l = Zx[jr * QW + xl], r = Zx[jr * QW + xr];
+            const T d = Zy[yd * QW + ir], u = Zy[yu * QW + ir];
+            const T dl = Zd[yd * QW + xl], dr = Zd[yd * QW + xr], ul = Zd[yu * QW + xl], ur = Zd[yu * QW + xr];
+            T* w = Zc + jr * QW + ir;
+            if (inner) {
+                *w = (Bc[jr * QW + ir] - (c.fc * (dl + dr + ul + ur) + c.fey * (d + u) + c.fex * (l + r))) *
+                     c.invd[1][1];
+            } else {
+                const int i = zx + ii, j = zy + jj;
+                if (unsigned(i) >= unsigned(M) || unsigned(j) >= unsigned(N)) continue;
+                *w = (Bc[jr * QW + ir] - fem_off_vals(c, i, j, dl, d, dr, l, r, ul, u, ur)) *
+                     c.invd[cls(i, M)][cls(j, N)];
+            }
+        }
+        __syncthreads();
+    }
+    auto zat = [&](int ii, int jj) -> T { return Z[qidx(ii, jj)]; };
+    auto resid = [&](int ii, int jj) -> T {
+        const int i = zx + ii, j = zy + jj;
+        T off = fem_off_vals(c, i, j, zat(ii - 1, jj - 1), zat(ii, jj - 1), zat(ii + 1, jj - 1), zat(ii - 1, jj),
+                             zat(ii + 1, jj), zat(ii - 1, jj + 1), zat(ii, jj + 1), zat(ii + 1, jj + 1));
+        return B[qidx(ii, jj)] - c.d[cls(i, M)][cls(j, N)] * zat(ii, jj) - off;
+    };
+    for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
+        const int j = zy + jj;
+        if (j >= N) break;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int ii = ZH + lane + 32 * h;
+            const int i = zx + ii;
+            if (ii < ZH + TX && i < M) a.zout[i + M * j] = zat(ii, jj);
+        }
+    }
+    if (MODE == 0) {
+        // residuals on the interior and one ring, then P^T onto coarse nodes
+        for (int jr = warp; jr < RH; jr += NW) {
+            const int jj = ZH - 1 + jr, j = zy + jj;
+            for (int ir = lane; ir < RW; ir += 32) {
+                const int ii = ZH - 1 + ir, i = zx + ii;
+                R[jr * RW + ir] = (unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N)) ? resid(ii, jj) : T(0);
+            }
+        }
+        __syncthreads();
+        const int Mc = (M - 1) / 2 + 1, Nc = (N - 1) / 2 + 1;
+        constexpr int CX = TX / 2, CY = TY / 2;
+        for (int t = threadIdx.x; t < CX * CY; t += G::NT) {
+            const int q = t / CX;
+            const int I = x0 / 2 + (t - q * CX), J = y0 / 2 + q;
+            if (I >= Mc || J >= Nc) continue;
+            a.bc[I + Mc * J] = fem_restrict_at(M, N, R, RW, x0 - 1, y0 - 1, I, J);
+        }
+    } else if (a.norm) {
+        double s = 0;
+        for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
+            const int j = zy + jj;
+            if (j >= N) break;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int ii = ZH + lane + 32 * h;
+                if (ii < ZH + TX && zx + ii < M) {
+                    double r = double(resid(ii, jj));
+                    s += r * r;
+                }
+            }
+        }
+        s = block_sum(s);
+        double total;
+        if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
+    }
+}
+
 // ---------------------------------------------------- CTA-resident levels
 template <typename T>
 struct CCStack {
@@ -924,6 +1086,21 @@ static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T>& a
     cc_tile<T, MODE, 2><<<grid, G::NT, G::smem, s>>>(c, a);
 }
 
+template <typename T, int MODE>
+static void launch_fem_tile(cudaStream_t s, const FEMc<T>& c, const TileArgs<T>& a) {
+    using G = FEMTile<T>;
+    dim3 grid((c.M + G::TX - 1) / G::TX, (c.N + G::TY - 1) / G::TY);
+    fem_tile<T, MODE><<<grid, G::NT, G::smem, s>>>(c, a);
+}
+
+template <typename T>
+static cudaError_t fem_tile_attr() {
+    using G = FEMTile<T>;
+    cudaError_t e = cudaFuncSetAttribute(fem_tile<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fem_tile<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+}
+
 template <typename T>
 static cudaError_t cc_tile_attr() {
     using G = CCTile<T, 2>;
@@ -1151,6 +1328,8 @@ class MG {
         VDI_CUDA((tile_attr<float, 1, 1, FEMc<float>>()));
         VDI_CUDA(cc_tile_attr<double>());
         VDI_CUDA(cc_tile_attr<float>());
+        VDI_CUDA(fem_tile_attr<double>());
+        VDI_CUDA(fem_tile_attr<float>());
         return VDI_OK;
     }
 
@@ -1220,7 +1399,7 @@ class MG {
         TileArgs<T> a = targs<T>(z, zs_tmp, b);
         a.zero_init = zero_init;
         a.bc = bs[l + 1];
-        if (fem()) launch_tile<T, 1, 0>(s, femc<T>(l), a, lv[l].m, lv[l].n);
+        if (fem()) launch_fem_tile<T, 0>(s, femc<T>(l), a);
         else launch_cc_tile<T, 0>(s, ccc<T>(l), a);
         VDI_CUDA(cudaGetLastError());
         VDI_TRY(vcycle<T>(s, l + 1, bs[l + 1], zs[l + 1], nmulti, zs, bs, smem, 1, 0, 0, 0));
@@ -1229,7 +1408,7 @@ class MG {
         p.norm = norm;
         p.use_cond = use_cond;
         p.h = h;
-        if (fem()) launch_tile<T, 1, 1>(s, femc<T>(l), p, lv[l].m, lv[l].n);
+        if (fem()) launch_fem_tile<T, 1>(s, femc<T>(l), p);
         else launch_cc_tile<T, 1>(s, ccc<T>(l), p);
         VDI_CUDA(cudaGetLastError());
         return VDI_OK;
@@ -1443,6 +1622,50 @@ int mg_residual(MG* mg, cudaStream_t s, const double* b, const double* z, double
     return VDI_OK;
 }
 
+int mg_kernels_per_iteration(const MG* mg, int precision) {
+    int nm = precision == VDI_MG_MIXED ? mg->nmulti32 : mg->nmulti64;
+    int k = 2 * nm + 1;                       // PRE/POST per tiled level + the coarsest
+    if (precision == VDI_MG_MIXED) k += 2;    // FP64 update and residual
+    else if (nm == 0) k += 1;                 // separate norm when no tile level exists
+    return k;
+}
+
+int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, double* z, float* ms, double* bytes) {
+    if (mg->nmulti64 < 1 || iters < 1) return VDI_ERR_INVALID_ARGUMENT;
+    cudaEvent_t e0, e1;
+    VDI_CUDA(cudaEventCreate(&e0));
+    VDI_CUDA(cudaEventCreate(&e1));
+    TileArgs<double> a = mg->targs<double>(which == 0 ? z : mg->t64[0], which == 0 ? mg->t64[0] : z, b);
+    a.bc = mg->b64[1];
+    a.zc = mg->z64[1];
+    auto launch = [&]() {
+        if (mg->fem()) {
+            if (which == 0) launch_fem_tile<double, 0>(s, mg->femc<double>(0), a);
+            else launch_fem_tile<double, 1>(s, mg->femc<double>(0), a);
+        } else {
+            if (which == 0) launch_cc_tile<double, 0>(s, mg->ccc<double>(0), a);
+            else launch_cc_tile<double, 1>(s, mg->ccc<double>(0), a);
+        }
+    };
+    // the coarse inputs of POST must hold numbers: one V-cycle fills them
+    VDI_TRY(mg->vcycle64(s, b, z, 0, 0, 0));
+    launch();
+    VDI_CUDA(cudaEventRecord(e0, s));
+    for (int k = 0; k < iters; k++) launch();
+    VDI_CUDA(cudaEventRecord(e1, s));
+    VDI_CUDA(cudaEventSynchronize(e1));
+    float t = 0;
+    VDI_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / iters;
+    // z in, b in, z out (8 bytes each per point) and the coarse array (8 bytes
+    // per coarse point, written by PRE, read by POST)
+    double N = double(mg->size(0)), Nc = double(mg->size(1));
+    *bytes = 3 * 8 * N + 8 * Nc;
+    return VDI_OK;
+}
+
 int mg_apply(MG* mg, cudaStream_t s, const double* z, double* y) {
     long N = mg->size(0);
     if (mg->fem())
@@ -1573,6 +1796,7 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
     if (e == cudaSuccess) e = tile_attr<double, 1, 0, FEMc<double>>();
     if (e == cudaSuccess) e = tile_attr<double, 1, 1, FEMc<double>>();
     if (e == cudaSuccess) e = cc_tile_attr<double>();
+    if (e == cudaSuccess) e = fem_tile_attr<double>();
     if (e != cudaSuccess) {
         set_error("vdi_mg_solve_noalloc: %s", cudaGetErrorString(e));
         forget();

@@ -40,6 +40,8 @@ struct vdi_sim {
     double* gas_work = nullptr;
     double *src_mac = nullptr, *q = nullptr, *q_prev = nullptr;
     double *src_fem = nullptr, *zf = nullptr, *zf_prev = nullptr;
+    // third-latest solutions for the quadratic initial guess
+    double *q_prev2 = nullptr, *zu_prev2 = nullptr, *zv_prev2 = nullptr, *zf_prev2 = nullptr;
     double *su = nullptr, *sv = nullptr, *zu = nullptr, *zu_prev = nullptr, *zv = nullptr, *zv_prev = nullptr;
     GuessHist* hist = nullptr;   // 4 entries
     double* d_time = nullptr;
@@ -82,6 +84,14 @@ int update_visc(vdi_sim* S, double dt) {
     return VDI_OK;
 }
 
+/** mgs_common::initial_guess (mgs_common.cc:17-50) for one solver, or the
+ * quadratic variant when the parameters ask for it. */
+int guess(vdi_sim* S, cudaStream_t s, int which, double* z, double* zp, double* zp2, int n) {
+    if (S->prm.mg_guess == VDI_GUESS_QUADRATIC)
+        return launch_guess2(s, z, zp, zp2, n, S->hist + which, S->d_time, S->d_err);
+    return launch_guess(s, z, zp, n, S->hist + which, S->d_time, S->d_err);
+}
+
 /** Enqueues one fluid_2d::step_forward(dt) (fluid_2d.cc:93-405). */
 int enqueue_step(vdi_sim* S, double dt) {
     const Grid& g = S->g;
@@ -99,7 +109,7 @@ int enqueue_step(vdi_sim* S, double dt) {
     VDI_TRY(launch_stage34(s, g, S->f, dt));
     VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
     VDI_TRY(launch_stage5_src(s, g, S->f, S->gas, dt, S->src_mac));
-    VDI_TRY(launch_guess(s, S->q, S->q_prev, mn, S->hist + SOLVER_MAC, S->d_time, S->d_err));
+    VDI_TRY(guess(S, s, SOLVER_MAC, S->q, S->q_prev, S->q_prev2, mn));
     VDI_TRY(mg_solve_device(S->mg[SOLVER_MAC], s, S->src_mac, S->q, prec));
     VDI_TRY(launch_mac_advect(s, g, S->f, S->gas, S->q, dt, S->d_time));
     VDI_TRY(launch_inviscid_bc(s, g, S->f, S->gas, dt));
@@ -115,9 +125,9 @@ int enqueue_step(vdi_sim* S, double dt) {
             VDI_CUDA(cudaEventRecord(S->ev_vy, s));
             VDI_CUDA(cudaStreamWaitEvent(S->s_vy, S->ev_vy, 0));
         }
-        VDI_TRY(launch_guess(s, S->zu, S->zu_prev, mn, S->hist + SOLVER_VX, S->d_time, S->d_err));
+        VDI_TRY(guess(S, s, SOLVER_VX, S->zu, S->zu_prev, S->zu_prev2, mn));
         VDI_TRY(mg_solve_device(S->mg[SOLVER_VX], s, S->su, S->zu, prec));
-        VDI_TRY(launch_guess(sv, S->zv, S->zv_prev, mn, S->hist + SOLVER_VY, S->d_time, S->d_err));
+        VDI_TRY(guess(S, sv, SOLVER_VY, S->zv, S->zv_prev, S->zv_prev2, mn));
         VDI_TRY(mg_solve_device(S->mg[SOLVER_VY], sv, S->sv, S->zv, prec));
         if (par) {
             VDI_CUDA(cudaEventRecord(S->ev_vy_done, S->s_vy));
@@ -130,7 +140,7 @@ int enqueue_step(vdi_sim* S, double dt) {
         c1v = CellView{S->f.fc1, m + 4, 2 * (m + 4) + 2};
     }
     VDI_TRY(launch_fem_rhs(s, g, S->f, S->gas, c0v, c1v, dt, S->fem_acc_edge, S->fem_acc_mid, S->src_fem));
-    VDI_TRY(launch_guess(s, S->zf, S->zf_prev, nf, S->hist + SOLVER_FEM, S->d_time, S->d_err));
+    VDI_TRY(guess(S, s, SOLVER_FEM, S->zf, S->zf_prev, S->zf_prev2, nf));
     VDI_TRY(mg_solve_device(S->mg[SOLVER_FEM], s, S->src_fem, S->zf, prec));
     VDI_TRY(launch_vel_update(s, g, S->f, c0v, c1v, S->zf, dt));
     VDI_TRY(launch_viscous_bc(s, g, S->f, S->gas));
@@ -364,14 +374,15 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     for (auto pp : gptrs3)
         if ((st = alloc_zero(S, pp, m)) != VDI_OK) return fail(st);
     if ((st = alloc_zero(S, &S->gas_work, gas_work_doubles(m))) != VDI_OK) return fail(st);
-    double** cells[] = {&S->src_mac, &S->q, &S->q_prev, &S->su, &S->sv, &S->zu, &S->zu_prev, &S->zv, &S->zv_prev};
+    double** cells[] = {&S->src_mac, &S->q,  &S->q_prev,  &S->su,      &S->sv,      &S->zu,
+                        &S->zu_prev, &S->zv, &S->zv_prev, &S->q_prev2, &S->zu_prev2, &S->zv_prev2};
     for (auto pp : cells)
         if ((st = alloc_zero(S, pp, mn)) != VDI_OK) return fail(st);
-    double** nodes[] = {&S->src_fem, &S->zf, &S->zf_prev};
+    double** nodes[] = {&S->src_fem, &S->zf, &S->zf_prev, &S->zf_prev2};
     for (auto pp : nodes)
         if ((st = alloc_zero(S, pp, nf)) != VDI_OK) return fail(st);
     double* misc;
-    if ((st = alloc_zero(S, &misc, 2 + 4 * 4)) != VDI_OK) return fail(st);
+    if ((st = alloc_zero(S, &misc, 2 + 4 * (sizeof(GuessHist) / 8 + 1))) != VDI_OK) return fail(st);
     S->d_time = misc;
     S->d_vframe = misc + 1;
     S->hist = reinterpret_cast<GuessHist*>(misc + 2);
@@ -420,10 +431,11 @@ static int reset_histories(vdi_sim* S) {
     cudaStream_t s = S->s;
     size_t mn = size_t(S->prm.m) * S->prm.n, nf = size_t(S->prm.m + 1) * (S->prm.n + 1);
     VDI_CUDA(cudaMemsetAsync(S->hist, 0, 4 * sizeof(GuessHist), s));
-    double* zs[] = {S->q, S->q_prev, S->zu, S->zu_prev, S->zv, S->zv_prev};
+    double* zs[] = {S->q, S->q_prev, S->zu, S->zu_prev, S->zv, S->zv_prev, S->q_prev2, S->zu_prev2, S->zv_prev2};
     for (auto z : zs) VDI_CUDA(cudaMemsetAsync(z, 0, mn * sizeof(double), s));
     VDI_CUDA(cudaMemsetAsync(S->zf, 0, nf * sizeof(double), s));
     VDI_CUDA(cudaMemsetAsync(S->zf_prev, 0, nf * sizeof(double), s));
+    VDI_CUDA(cudaMemsetAsync(S->zf_prev2, 0, nf * sizeof(double), s));
     return VDI_OK;
 }
 
@@ -547,6 +559,17 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
             VDI_CUDA(cudaMemcpy(mg_ctl(S->mg[k]), &c, sizeof(SolveCtl), cudaMemcpyHostToDevice));
         }
     }
+    // launches: per step the gas-layer update, the four stencil stages, the
+    // MAC correction, two boundary kernels, the FEM source, the velocity update
+    // and the final boundary kernel (+1 viscous source when implicit), two
+    // kernels per initial guess; per solve two set-up kernels and the first
+    // residual check; per solve-loop iteration the kernels of its V-cycle.
+    long launches = S->steps * (11 + (S->prm.implicit_visc ? 1 : 0));
+    for (int k = 0; k < 4; k++) {
+        if (!S->mg[k]) continue;
+        launches += out->solves[k] * (2 + 3) + out->vcycles[k] * mg_kernels_per_iteration(S->mg[k], S->prm.mg_precision);
+    }
+    out->kernel_launches = launches;
     GasStats gs;
     VDI_CUDA(cudaMemcpy(&gs, S->d_gstats, sizeof(gs), cudaMemcpyDeviceToHost));
     out->newton_steps = long(gs.newton_steps);
@@ -638,6 +661,13 @@ int vdi_mg_apply(vdi_mg* h, const double* d_z, double* d_y) {
     VDI_TRY(mg_apply(h->g, h->s, d_z, d_y));
     VDI_CUDA(cudaStreamSynchronize(h->s));
     return VDI_OK;
+}
+
+int vdi_mg_profile(vdi_mg* h, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
+                   double* bytes_per_launch) {
+    if (!h || !d_b || !d_z || !ms_per_launch || !bytes_per_launch || (which != 0 && which != 1))
+        return VDI_ERR_INVALID_ARGUMENT;
+    return mg_profile(h->g, h->s, which, iters, d_b, d_z, ms_per_launch, bytes_per_launch);
 }
 
 int vdi_tri_solve(int n, double* d_a, double* d_b, double* d_c, double* d_d, void* stream, int* pivoted) {

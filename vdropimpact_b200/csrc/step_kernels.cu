@@ -470,6 +470,54 @@ __global__ void k_guess_finish(GuessHist* h, const double* d_time, int* err) {
     }
 }
 
+/** Second-order variant of k_guess_apply: with three past solutions z (at
+ * t0), zprev (t_prev) and zprev2 (t_prev2) the guess is the quadratic
+ * Lagrange extrapolation to t; with two it is the linear rule above. This
+ * changes only the starting iterate of the solve, not its converged result. */
+__global__ void k_guess2_apply(double* __restrict__ z, double* __restrict__ zprev, double* __restrict__ zprev2, int n,
+                               const GuessHist* h, const double* d_time) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int sc = h->scount;
+    if (sc < 2) {
+        if (sc == 1) zprev[k] = z[k];
+        return;
+    }
+    double t = *d_time, t0 = h->t0, t1 = h->t_prev;
+    if (fabs(t0 - t1) < 2.220446049250313e-16 * 10) return;
+    double zz = z[k];
+    if (sc == 2) {
+        double a = 1. / (t0 - t1), b = (t - t1) * a, cc = (t - t0) * a;
+        z[k] = b * zz - cc * zprev[k];
+    } else {
+        double t2 = h->t_prev2;
+        double l0 = (t - t1) * (t - t2) / ((t0 - t1) * (t0 - t2));
+        double l1 = (t - t0) * (t - t2) / ((t1 - t0) * (t1 - t2));
+        double l2 = (t - t0) * (t - t1) / ((t2 - t0) * (t2 - t1));
+        z[k] = l0 * zz + l1 * zprev[k] + l2 * zprev2[k];
+    }
+    zprev2[k] = zprev[k];
+    zprev[k] = zz;
+}
+
+__global__ void k_guess2_finish(GuessHist* h, const double* d_time, int* err) {
+    double t = *d_time;
+    if (h->scount < 2) {
+        if (h->scount == 1) h->t0 = t;
+        else h->t_prev = t;
+        h->scount++;
+    } else {
+        if (fabs(h->t0 - h->t_prev) < 2.220446049250313e-16 * 10) {
+            atomicOr(err, DEV_DUP_TIME);
+            return;
+        }
+        h->t_prev2 = h->t_prev;
+        h->t_prev = h->t0;
+        h->t0 = t;
+        if (h->scount < 3) h->scount++;
+    }
+}
+
 // --------------------------------------------------------------- launch
 static dim3 cell_grid(int m, int n) { return dim3((m + 31) / 32, (n + 7) / 8); }
 static const dim3 CELL_BLOCK(32, 8);
@@ -519,6 +567,13 @@ int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c
     k_vel_update<<<cell_grid(g.m + 1, g.n + 1), CELL_BLOCK, 0, s>>>(g, f, c0, c1, z, dt);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
+int launch_guess2(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,
+                  const double* d_time, int* err) {
+    k_guess2_apply<<<(n + 255) / 256, 256, 0, s>>>(z, zprev, zprev2, n, h, d_time);
+    k_guess2_finish<<<1, 1, 0, s>>>(h, d_time, err);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+
 int launch_guess(cudaStream_t s, double* z, double* zprev, int n, GuessHist* h, const double* d_time, int* err) {
     k_guess_apply<<<(n + 255) / 256, 256, 0, s>>>(z, zprev, n, h, d_time);
     k_guess_finish<<<1, 1, 0, s>>>(h, d_time, err);

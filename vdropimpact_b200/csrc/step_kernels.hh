@@ -51,6 +51,7 @@ struct GasStats {
 struct GuessHist {
     int scount;
     double t_prev, t0;
+    double t_prev2;     // time of the third-latest solution (quadratic guess)
 };
 
 /** A read-only view of a cell array with an arbitrary pitch and origin. */
@@ -75,6 +76,10 @@ int launch_fem_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs
 int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c0, CellView c1, const double* z,
                       double dt);
 int launch_guess(cudaStream_t s, double* z, double* zprev, int n, GuessHist* h, const double* d_time, int* err);
+/** Quadratic-in-time extrapolation from the last three solutions (zprev2 the
+ * oldest); falls back to the reference's linear rule until three exist. */
+int launch_guess2(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,
+                  const double* d_time, int* err);
 
 /** Gas-layer update (gas_layer::update, gas_layer.cc:36-46) as one CTA.
  * Also advances *d_time by dt/2 (fluid_2d.cc:102). */

@@ -113,5 +113,10 @@ int mg_configure(MG* mg, double rtol, int max_it);
 /** Builds the conditional-node loop for the solve into a graph under
  * stream capture. Returns VDI_OK when a graph loop was recorded. */
 int mg_record_graph_solve(MG* mg, cudaStream_t s, const double* b, double* z, int precision);
+/** Kernel launches of one solve-loop iteration (a V-cycle and its norm). */
+int mg_kernels_per_iteration(const MG* mg, int precision);
+/** Times the finest-level PRE (which=0) or POST (which=1) kernel. */
+int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, double* z, float* ms,
+               double* bytes);
 
 }  // namespace vdi
