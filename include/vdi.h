@@ -139,7 +139,8 @@ typedef struct vdi_stats {
 int vdi_sim_stats(vdi_sim* sim, vdi_stats* out, int reset);
 
 /* Device pointers to the state arrays (read-only use by callers that keep
- * data on the device). which: 0 u, 1 v, 2 p, 3 gas h, 4 gas pg, 5 gas gp. */
+ * data on the device). which: 0 u, 1 v, 2 p, 3 gas h, 4 gas pg, 5 gas gp,
+ * 6 the last MAC source, 7 the last MAC solution (m*n each). */
 int vdi_sim_device_field(vdi_sim* sim, int which, double** d_ptr, size_t* count);
 
 /* --------------------------------------------------------- multigrid
@@ -180,6 +181,32 @@ int vdi_mg_apply(vdi_mg* mg, const double* d_z, double* d_y);
  * array read or written once). */
 int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
                    double* bytes_per_launch);
+
+/* ------------------------------------------------------------ U-Net
+ * The learned initial guess has no counterpart in the reference. A small
+ * convolutional U-Net maps the RMS-normalised residual of the extrapolated
+ * guess, on a coarsened H x W grid (H a multiple of 8, W of 16), to a
+ * normalised correction. Inputs and outputs are FP32 device arrays of batch
+ * x H x W values; parameters are BF16 on the device with FP32 master copies. */
+typedef struct vdi_unet vdi_unet;
+int vdi_unet_create(int H, int W, int batch, unsigned seed, void* stream, vdi_unet** out);
+int vdi_unet_destroy(vdi_unet* net);
+long vdi_unet_param_count(const vdi_unet* net);
+int vdi_unet_forward(vdi_unet* net, const float* d_in, float* d_out, int batch);
+/* One Adam step on the mean squared error of the output against d_target. */
+int vdi_unet_train_step(vdi_unet* net, const float* d_in, const float* d_target, int batch, float lr, float* h_loss);
+/* Loss and the weight gradient of one layer ([9][cout][cin], FP32) without
+ * updating the parameters (gradient checks). */
+int vdi_unet_gradients(vdi_unet* net, const float* d_in, const float* d_target, int batch, int layer, float* h_grad,
+                       float* h_loss);
+/* All parameters (per layer: weights [9][cout][cin], then biases), FP32, to
+ * (to_device = 1) or from the device. */
+int vdi_unet_params(vdi_unet* net, float* h_buf, long count, int to_device);
+/* Attaches a trained network to the MAC solve of a simulation as its
+ * VDI_GUESS_LEARNED initial guess: the network runs on the residual of the
+ * extrapolated guess restricted by factor (2 or 4), and its output times
+ * out_scale * rms(residual) / xxsp, prolonged back, is added to the guess. */
+int vdi_sim_attach_unet(vdi_sim* sim, vdi_unet* net, int factor, double out_scale);
 
 /* vdi_mg_solve_noalloc has no counterpart in the reference. It is the FP64
  * solve of vdi_mg_create + vdi_mg_solve for callers that must not allocate

@@ -175,6 +175,12 @@ class Fluid2D:
                     height_fixed_point_iters=s.height_fixed_point_iters,
                     last_rel_res=dict(zip(names, list(s.last_rel_res))), kernel_launches=s.kernel_launches)
 
+    def attach_unet(self, net, factor: int):
+        """Uses net (learned.UNet, trained on this grid restricted by factor)
+        as the MAC solve's learned initial-guess correction."""
+        check(lib().vdi_sim_attach_unet(self._h, net._h, factor, float(net.out_scale)), "vdi_sim_attach_unet")
+        self._unet = net
+
     def device_field(self, which: int):
         p = _abi._dp()
         n = C.c_size_t()

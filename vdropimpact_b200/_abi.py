@@ -111,6 +111,16 @@ _SIGS = [
     ("vdi_mg_apply", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("vdi_mg_profile", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_float),
                                  _dp]),
+    ("vdi_unet_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint, C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("vdi_unet_destroy", C.c_int, [C.c_void_p]),
+    ("vdi_unet_param_count", C.c_long, [C.c_void_p]),
+    ("vdi_unet_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    ("vdi_unet_train_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                      C.POINTER(C.c_float)]),
+    ("vdi_unet_gradients", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                     C.POINTER(C.c_float)]),
+    ("vdi_unet_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_int]),
+    ("vdi_sim_attach_unet", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double]),
     ("vdi_tri_solve", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.POINTER(C.c_int)]),
 ]

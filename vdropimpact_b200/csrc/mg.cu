@@ -1666,6 +1666,16 @@ int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, do
     return VDI_OK;
 }
 
+int mg_residual_async(MG* mg, cudaStream_t s, const double* b, const double* z, double* r, double* d_norm) {
+    int nb = rblocks(mg->size(0));
+    if (mg->fem())
+        resid_out_k<double><<<nb, 256, 0, s>>>(mg->femc<double>(0), z, b, r, mg->rd, d_norm);
+    else
+        resid_out_k<double><<<nb, 256, 0, s>>>(mg->ccc<double>(0), z, b, r, mg->rd, d_norm);
+    VDI_CUDA(cudaGetLastError());
+    return VDI_OK;
+}
+
 int mg_apply(MG* mg, cudaStream_t s, const double* z, double* y) {
     long N = mg->size(0);
     if (mg->fem())

@@ -57,6 +57,13 @@ struct vdi_sim {
     cudaGraphExec_t gexec = nullptr;
     double graph_dt = 0;
     long steps = 0;
+    // learned initial guess of the MAC solve
+    vdi_unet* unet = nullptr;
+    int unet_factor = 0;
+    double unet_scale = 0;
+    double* unet_r = nullptr;      // residual of the extrapolated guess (m x n)
+    double* unet_norm = nullptr;   // its 2-norm
+    float *unet_in = nullptr, *unet_out = nullptr;
 };
 
 namespace {
@@ -87,7 +94,7 @@ int update_visc(vdi_sim* S, double dt) {
 /** mgs_common::initial_guess (mgs_common.cc:17-50) for one solver, or the
  * quadratic variant when the parameters ask for it. */
 int guess(vdi_sim* S, cudaStream_t s, int which, double* z, double* zp, double* zp2, int n) {
-    if (S->prm.mg_guess == VDI_GUESS_QUADRATIC)
+    if (S->prm.mg_guess == VDI_GUESS_QUADRATIC || S->prm.mg_guess == VDI_GUESS_LEARNED)
         return launch_guess2(s, z, zp, zp2, n, S->hist + which, S->d_time, S->d_err);
     return launch_guess(s, z, zp, n, S->hist + which, S->d_time, S->d_err);
 }
@@ -110,6 +117,16 @@ int enqueue_step(vdi_sim* S, double dt) {
     VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
     VDI_TRY(launch_stage5_src(s, g, S->f, S->gas, dt, S->src_mac));
     VDI_TRY(guess(S, s, SOLVER_MAC, S->q, S->q_prev, S->q_prev2, mn));
+    if (S->prm.mg_guess == VDI_GUESS_LEARNED) {
+        // the network corrects the extrapolated guess from its residual
+        if (!S->unet) {
+            set_error("VDI_GUESS_LEARNED needs a network (vdi_sim_attach_unet)");
+            return VDI_ERR_NOT_READY;
+        }
+        VDI_TRY(mg_residual_async(S->mg[SOLVER_MAC], s, S->src_mac, S->q, S->unet_r, S->unet_norm));
+        VDI_TRY(unet_correct(S->unet, s, S->unet_r, S->unet_norm, S->q, m, n, S->unet_factor, S->unet_scale,
+                             S->unet_in, S->unet_out));
+    }
     VDI_TRY(mg_solve_device(S->mg[SOLVER_MAC], s, S->src_mac, S->q, prec));
     VDI_TRY(launch_mac_advect(s, g, S->f, S->gas, S->q, dt, S->d_time));
     VDI_TRY(launch_inviscid_bc(s, g, S->f, S->gas, dt));
@@ -409,6 +426,39 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     return VDI_OK;
 }
 
+int vdi_sim_attach_unet(vdi_sim* S, vdi_unet* net, int factor, double out_scale) {
+    if (!S || !net || (factor != 1 && factor != 2 && factor != 4 && factor != 8)) return VDI_ERR_INVALID_ARGUMENT;
+    int H, W;
+    unet_dims(net, &H, &W);
+    if (S->prm.m / factor != W || S->prm.n / factor != H || S->prm.m % factor || S->prm.n % factor) {
+        set_error("vdi_sim_attach_unet: the network grid %dx%d does not match %dx%d / %d", W, H, S->prm.m,
+                  S->prm.n, factor);
+        return VDI_ERR_INVALID_ARGUMENT;
+    }
+    if (!S->unet_r) {
+        int st;
+        if ((st = alloc_zero(S, &S->unet_r, size_t(S->prm.m) * S->prm.n)) != VDI_OK) return st;
+        if ((st = alloc_zero(S, &S->unet_norm, 1)) != VDI_OK) return st;
+        double* f;
+        if ((st = alloc_zero(S, &f, size_t(H) * W)) != VDI_OK) return st;   // 2 float arrays
+        S->unet_in = reinterpret_cast<float*>(f);
+        S->unet_out = S->unet_in + size_t(H) * W;
+    }
+    S->unet = net;
+    S->unet_factor = factor;
+    // scale of the output: out_scale * rms(r) / xxsp
+    S->unet_scale = out_scale / S->g.xxsp;
+    destroy_graph(S);
+    // one eager correction on zeros sets the kernels' shared-memory limits
+    // before any stream capture
+    VDI_CUDA(cudaMemsetAsync(S->unet_r, 0, sizeof(double) * S->prm.m * S->prm.n, S->s));
+    VDI_CUDA(cudaMemsetAsync(S->unet_norm, 0, sizeof(double), S->s));
+    VDI_TRY(unet_correct(net, S->s, S->unet_r, S->unet_norm, S->unet_r, S->prm.m, S->prm.n, factor, 0.,
+                         S->unet_in, S->unet_out));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    return VDI_OK;
+}
+
 int vdi_sim_destroy(vdi_sim* S) {
     if (!S) return VDI_OK;
     if (S->s) cudaStreamSynchronize(S->s);
@@ -592,6 +642,8 @@ int vdi_sim_device_field(vdi_sim* S, int which, double** d_ptr, size_t* count) {
         case 3: *d_ptr = S->gas.h; if (count) *count = m; break;
         case 4: *d_ptr = S->gas.pg; if (count) *count = m + 1; break;
         case 5: *d_ptr = S->gas.gp; if (count) *count = m + 1; break;
+        case 6: *d_ptr = S->src_mac; if (count) *count = size_t(m) * S->prm.n; break;
+        case 7: *d_ptr = S->q; if (count) *count = size_t(m) * S->prm.n; break;
         default: return VDI_ERR_INVALID_ARGUMENT;
     }
     return VDI_OK;

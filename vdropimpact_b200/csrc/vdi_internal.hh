@@ -119,4 +119,15 @@ int mg_kernels_per_iteration(const MG* mg, int precision);
 int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, double* z, float* ms,
                double* bytes);
 
+/** r = b - A z on the finest level and ||r||_2 into *d_norm, on the stream
+ * without host synchronisation (graph-capturable). */
+int mg_residual_async(MG* mg, cudaStream_t s, const double* b, const double* z, double* r, double* d_norm);
+
+/** Learned correction of an initial guess: restricts r (m x n) by factor,
+ * normalises by its RMS (from d_rnorm = ||r||_2), runs the U-Net and adds
+ * scale * rms * (prolonged output) to z. in_buf/out_buf hold H x W floats. */
+int unet_correct(vdi_unet* u, cudaStream_t s, const double* r, const double* d_rnorm, double* z, int m, int n,
+                 int factor, double scale, float* in_buf, float* out_buf);
+int unet_dims(const vdi_unet* u, int* H, int* W);
+
 }  // namespace vdi
