@@ -143,6 +143,44 @@ int vdi_sim_stats(vdi_sim* sim, vdi_stats* out, int reset);
  * 6 the last MAC source, 7 the last MAC solution (m*n each). */
 int vdi_sim_device_field(vdi_sim* sim, int which, double** d_ptr, size_t* count);
 
+/* ------------------------------------------------------ lift-off search
+ * The reference's analysis tool (tt_analysis.cc:97-171) run on the device
+ * after every step: the minimum of the gas-layer height profile (as the
+ * float32 values a frame file holds, gas_layer_solve.cc:258-282), Gaussian
+ * smoothed and interpolated by cubic Hermite pieces (the tool's default) or
+ * raw (its -r flag), and the search for the global minimum height, closed
+ * once a later minimum exceeds it by 0.5%. The initial state is state 0;
+ * state k follows step k*every. On by default (smoothed, every step, no
+ * history); init_fields and set_state restart it. */
+enum vdi_liftoff_mode {
+    VDI_LIFTOFF_OFF = 0,
+    VDI_LIFTOFF_SMOOTHED = 1,
+    VDI_LIFTOFF_RAW = 2
+};
+/* Sets the mode, the number of steps between analysed states (every = the
+ * frame's step count analyses frames) and the number of states whose
+ * (x, height) minimum is kept on the device; restarts the search. */
+int vdi_sim_liftoff_setup(vdi_sim* sim, int mode, int every, long history);
+typedef struct vdi_liftoff {
+    long states;              /* states analysed */
+    long min_state;           /* the state of the global minimum (lift-off), -1 before any */
+    double min_height, min_x; /* that minimum and its position */
+    double interval;          /* time between analysed states (dt * every) */
+    double t_rel;             /* min_state * interval - h0 / V (tt_analysis.cc:169-171) */
+    double t_rel_ev;          /* min_state * interval - evanescent-field origin */
+    double percent;           /* 100 * min_state / (states - 1) */
+    int searching;            /* 1 while no later minimum exceeded the global one by 0.5% */
+    int ev_found;             /* 1 once a minimum fell below 500 nm (tt_analysis.cc:155-158) */
+    double last_x, last_height; /* the last analysed state's minimum */
+} vdi_liftoff;
+/* Reads the search; h_xmin/h_fmin (may be NULL when cap = 0) receive the
+ * first min(cap, states, history) per-state minima. */
+int vdi_sim_liftoff(vdi_sim* sim, vdi_liftoff* out, double* h_xmin, double* h_fmin, long cap);
+/* The per-profile part alone: the minimum (position, height) of one height
+ * profile d_h[m] on cells x_i = ax + (i+1/2) dx (tt_analysis.cc:111-146). */
+int vdi_profile_min(int m, double ax, double dx, int mode, const double* d_h, void* stream, double* h_xmin,
+                    double* h_fmin);
+
 /* --------------------------------------------------------- multigrid
  * A standalone linear system with the TGMG-style interface the reference's
  * problem classes use (mgs_mac.hh, mgs_fem.hh, visco_impl.hh). */

@@ -20,6 +20,11 @@
 //                                       as mg_test.cc:20-35 does
 //   visc <cfg> <vfx> <vfy> <horiz> <b> <z>  visco_impl::setup_and_solve
 //                                       (visco_impl.cc:21-39)
+//   heights <cfg> <nsteps> <out>        from init_fields, nsteps steps; writes
+//                                       for steps 0..nsteps the time and the
+//                                       gas-layer height h[m], the per-step
+//                                       input of the lift-off analysis
+//                                       (tt_analysis.cc:97-164)
 //   tri  <n> <abcd> <out> [thomas]      tri_solve::solve_lapack
 //                                       (tri_solve.cc:24-33) or solve()
 //                                       (tri_solve.cc:37-49)
@@ -151,6 +156,28 @@ static int run_steps(int argc,char** argv,bool dump,bool timed) {
     return 0;
 }
 
+static void height_row(fluid_2d& f,std::vector<double>& rows) {
+    gas_layer_solve* g=gls(f);
+    rows.push_back(f.time);
+    rows.insert(rows.end(),g->h,g->h+f.m);
+}
+
+static int run_heights(char** argv) {
+    fluid_2d f(argv[2]);
+    int nsteps=atoi(argv[3]);
+    f.init_fields();
+    double dt=frame_dt(f);
+    std::vector<double> rows;
+    height_row(f,rows);
+    for(int k=1;k<=nsteps;k++) {
+        f.step_forward(dt);
+        height_row(f,rows);
+    }
+    write_doubles(argv[4],&rows[0],rows.size());
+    printf("{\"steps\": %d, \"dt\": %.17g}\n",nsteps,dt);
+    return 0;
+}
+
 template<class T>
 static int solve_one(T& msu,const char* zfile) {
     msu.mg.setup();
@@ -167,6 +194,7 @@ int main(int argc,char** argv) {
     if(strcmp(cmd,"step")==0&&argc>=5) return run_steps(argc,argv,false,false);
     if(strcmp(cmd,"dump")==0&&argc>=6) return run_steps(argc,argv,true,false);
     if(strcmp(cmd,"time")==0&&argc>=4) return run_steps(argc,argv,false,true);
+    if(strcmp(cmd,"heights")==0&&argc>=5) return run_heights(argv);
     if((strcmp(cmd,"mac")==0||strcmp(cmd,"fem")==0)&&argc>=8) {
         int m=atoi(argv[2]),n=atoi(argv[3]);
         double dx=atof(argv[4]),dy=atof(argv[5]);

@@ -175,6 +175,29 @@ class Fluid2D:
                     height_fixed_point_iters=s.height_fixed_point_iters,
                     last_rel_res=dict(zip(names, list(s.last_rel_res))), kernel_launches=s.kernel_launches)
 
+    LIFTOFF = {"off": 0, "smoothed": 1, "raw": 2}
+
+    def liftoff_setup(self, mode="smoothed", every: int = 1, history: int = 0):
+        """Configures the device lift-off search (tt_analysis.cc:97-171):
+        mode "smoothed" (the tool's default), "raw" (its -r flag) or "off";
+        a state every `every` steps; `history` per-state minima kept."""
+        check(lib().vdi_sim_liftoff_setup(self._h, self.LIFTOFF[mode], every, history), "vdi_sim_liftoff_setup")
+        self._lhist = history
+
+    def liftoff(self) -> dict:
+        """The search so far: the lift-off state and its minimum, the tool's
+        summary times, and the per-state minima kept (xmin, hmin arrays)."""
+        out = _abi.VdiLiftoff()
+        cap = getattr(self, "_lhist", 0)
+        xs = np.zeros(max(cap, 1))
+        fs = np.zeros(max(cap, 1))
+        check(lib().vdi_sim_liftoff(self._h, C.byref(out), xs.ctypes.data_as(C.c_void_p),
+                                    fs.ctypes.data_as(C.c_void_p), cap), "vdi_sim_liftoff")
+        n = min(cap, out.states)
+        d = {k: getattr(out, k) for k, *_ in out._fields_}
+        d["xmin"], d["hmin"] = xs[:n].copy(), fs[:n].copy()
+        return d
+
     def attach_unet(self, net, factor: int):
         """Uses net (learned.UNet, trained on this grid restricted by factor)
         as the MAC solve's learned initial-guess correction."""
@@ -186,6 +209,19 @@ class Fluid2D:
         n = C.c_size_t()
         check(lib().vdi_sim_device_field(self._h, which, C.byref(p), C.byref(n)), "vdi_sim_device_field")
         return C.cast(p, C.c_void_p).value, n.value
+
+
+def profile_min(h, ax: float, dx: float, mode: str = "smoothed"):
+    """(x, height) of the minimum of one height profile (a float64 CUDA
+    tensor of m cell values) as the reference's analysis tool finds it
+    (tt_analysis.cc:111-146)."""
+    torch = _torch()
+    h = h.contiguous()
+    xm, fm = C.c_double(), C.c_double()
+    torch.cuda.synchronize()
+    check(lib().vdi_profile_min(h.numel(), ax, dx, Fluid2D.LIFTOFF[mode], C.c_void_p(h.data_ptr()), None,
+                                C.byref(xm), C.byref(fm)), "vdi_profile_min")
+    return xm.value, fm.value
 
 
 class _MgSystem:

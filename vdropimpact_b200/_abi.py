@@ -30,6 +30,10 @@ VDI_GUESS_EXTRAPOLATE = 0
 VDI_GUESS_LEARNED = 1
 VDI_GUESS_QUADRATIC = 2
 
+VDI_LIFTOFF_OFF = 0
+VDI_LIFTOFF_SMOOTHED = 1
+VDI_LIFTOFF_RAW = 2
+
 VDI_MG_MAC = 0
 VDI_MG_FEM = 1
 VDI_MG_VISC_U = 2
@@ -67,6 +71,13 @@ class VdiMgResult(C.Structure):
     _fields_ = [("vcycles", C.c_int), ("rel_res", C.c_double)]
 
 
+class VdiLiftoff(C.Structure):
+    _fields_ = [("states", C.c_long), ("min_state", C.c_long), ("min_height", C.c_double), ("min_x", C.c_double),
+                ("interval", C.c_double), ("t_rel", C.c_double), ("t_rel_ev", C.c_double), ("percent", C.c_double),
+                ("searching", C.c_int), ("ev_found", C.c_int), ("last_x", C.c_double),
+                ("last_height", C.c_double)]
+
+
 class VdiError(RuntimeError):
     def __init__(self, status: int, where: str, detail: str):
         super().__init__(f"{where}: status {status} ({_status_string(status)}): {detail}")
@@ -100,6 +111,9 @@ _SIGS = [
     ("vdi_sim_set_state", C.c_int, [C.c_void_p, C.POINTER(VdiState)]),
     ("vdi_sim_stats", C.c_int, [C.c_void_p, C.POINTER(VdiStats), C.c_int]),
     ("vdi_sim_device_field", C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(C.c_size_t)]),
+    ("vdi_sim_liftoff_setup", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_long]),
+    ("vdi_sim_liftoff", C.c_int, [C.c_void_p, C.POINTER(VdiLiftoff), C.c_void_p, C.c_void_p, C.c_long]),
+    ("vdi_profile_min", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p, _dp, _dp]),
     ("vdi_mg_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_void_p,
                                 C.POINTER(C.c_void_p)]),
     ("vdi_mg_destroy", C.c_int, [C.c_void_p]),

@@ -22,8 +22,8 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
                  "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 # Stencil and gas-layer kernels follow the reference's expression order
 # exactly; FMA contraction would change their rounding.
-EXACT = {"step_kernels.cu", "gas.cu"}
-SOURCES = ["mg.cu", "step_kernels.cu", "gas.cu", "sim.cu", "unet.cu", "batch.cu", "host_api.cu"]
+EXACT = {"step_kernels.cu", "gas.cu", "liftoff.cu"}
+SOURCES = ["mg.cu", "step_kernels.cu", "gas.cu", "liftoff.cu", "sim.cu", "unet.cu", "batch.cu", "host_api.cu"]
 
 
 def _sources():

@@ -1,7 +1,9 @@
 // The step driver (fluid_2d, fluid_2d.cc:14-405) over the device kernels,
 // and the C ABI declared in include/vdi.h.
 #include "step_kernels.hh"
+#include "liftoff.hh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -64,6 +66,11 @@ struct vdi_sim {
     double* unet_r = nullptr;      // residual of the extrapolated guess (m x n)
     double* unet_norm = nullptr;   // its 2-norm
     float *unet_in = nullptr, *unet_out = nullptr;
+    // lift-off search (tt_analysis.cc:97-171) after every step
+    LiftoffCfg lcfg{};
+    LiftoffState* d_lift = nullptr;
+    double2* d_lhist = nullptr;
+    long lcap = 0;
 };
 
 namespace {
@@ -110,6 +117,9 @@ int enqueue_step(vdi_sim* S, double dt) {
     VDI_CUDA(cudaStreamWaitEvent(S->s_gas, S->ev_fork, 0));
     VDI_TRY(launch_gas_update(S->s_gas, S->gp, S->gas, S->f.u, S->f.v, m + 4, S->d_vframe, dt, S->d_time,
                               S->gas_work, S->d_err, S->d_gstats));
+    // h is final for this step once the gas layer has updated it
+    if (S->lcfg.mode != VDI_LIFTOFF_OFF)
+        VDI_TRY(liftoff_launch(S->s_gas, S->gas.h, S->lcfg, S->d_lift, S->d_lhist, S->lcap, dt));
     VDI_CUDA(cudaEventRecord(S->ev_gas, S->s_gas));
     VDI_TRY(launch_stage1(s, g, S->f, dt));
     VDI_TRY(launch_stage2(s, g, S->f));
@@ -418,6 +428,12 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     for (int k = 0; k < 4; k++)
         if (S->mg[k] && (st = mg_configure(S->mg[k], S->prm.mg_rtol, S->prm.mg_max_vcycles)) != VDI_OK)
             return fail(st);
+    double* lbuf;
+    if ((st = alloc_zero(S, &lbuf, sizeof(LiftoffState) / 8 + 1)) != VDI_OK) return fail(st);
+    S->d_lift = reinterpret_cast<LiftoffState*>(lbuf);
+    if (P.m <= LIFTOFF_MAX_M &&
+        liftoff_config(P.m, P.ax, gp.dx, VDI_LIFTOFF_SMOOTHED, 1, P.R, P.V, &S->lcfg) != VDI_OK)
+        S->lcfg.mode = VDI_LIFTOFF_OFF;
     // mgs_fem::a_cc on the bottom row (mgs_fem.hh:55-57)
     double dydx = g.dy / g.dx, dxdy = g.dx / g.dy, fm = 4. / 3. * (dxdy + dydx);
     S->fem_acc_edge = 0.5 * 0.5 * fm;
@@ -477,6 +493,14 @@ int vdi_sim_destroy(vdi_sim* S) {
     return VDI_OK;
 }
 
+/** Restarts the lift-off search with the current state as state 0. */
+static int liftoff_restart(vdi_sim* S) {
+    VDI_TRY(liftoff_reset_async(S->s, S->d_lift));
+    if (S->lcfg.mode != VDI_LIFTOFF_OFF)
+        VDI_TRY(liftoff_launch(S->s, S->gas.h, S->lcfg, S->d_lift, S->d_lhist, S->lcap, 0.));
+    return VDI_OK;
+}
+
 static int reset_histories(vdi_sim* S) {
     cudaStream_t s = S->s;
     size_t mn = size_t(S->prm.m) * S->prm.n, nf = size_t(S->prm.m + 1) * (S->prm.n + 1);
@@ -503,6 +527,7 @@ int vdi_sim_init_fields(vdi_sim* S) {
     VDI_TRY(launch_gas_init(s, S->gp, S->gas, S->prm.h0, S->prm.V));
     VDI_TRY(launch_inviscid_bc(s, S->g, S->f, S->gas, 0.));
     VDI_TRY(launch_viscous_bc(s, S->g, S->f, S->gas));
+    VDI_TRY(liftoff_restart(S));
     VDI_CUDA(cudaStreamSynchronize(s));
     return VDI_OK;
 }
@@ -587,7 +612,67 @@ int vdi_sim_set_state(vdi_sim* S, const vdi_state* h) {
     hx[m] = hx[m - 1];
     VDI_CUDA(cudaMemcpy(S->gas.hx, hx.data(), (m + 1) * 8, cudaMemcpyHostToDevice));
     VDI_TRY(reset_histories(S));
+    VDI_TRY(liftoff_restart(S));
     VDI_CUDA(cudaStreamSynchronize(S->s));
+    return VDI_OK;
+}
+
+int vdi_sim_liftoff_setup(vdi_sim* S, int mode, int every, long history) {
+    if (!S || history < 0) return VDI_ERR_INVALID_ARGUMENT;
+    LiftoffCfg c{};
+    if (mode != VDI_LIFTOFF_OFF)
+        VDI_TRY(liftoff_config(S->prm.m, S->prm.ax, S->gp.dx, mode, every, S->prm.R, S->prm.V, &c));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    destroy_graph(S);
+    if (S->d_lhist) {
+        for (auto& p : S->bufs)
+            if (p == reinterpret_cast<double*>(S->d_lhist)) p = nullptr;
+        VDI_CUDA(cudaFree(S->d_lhist));
+        S->d_lhist = nullptr;
+    }
+    S->lcap = 0;
+    if (history > 0) {
+        double* hb;
+        VDI_TRY(alloc_zero(S, &hb, 2 * size_t(history)));
+        S->d_lhist = reinterpret_cast<double2*>(hb);
+        S->lcap = history;
+    }
+    S->lcfg = c;
+    S->lcfg.mode = mode;
+    VDI_TRY(liftoff_restart(S));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    return VDI_OK;
+}
+
+int vdi_sim_liftoff(vdi_sim* S, vdi_liftoff* out, double* h_xmin, double* h_fmin, long cap) {
+    if (!S || !out || cap < 0 || (cap > 0 && (!h_xmin || !h_fmin))) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    LiftoffState st;
+    VDI_CUDA(cudaMemcpy(&st, S->d_lift, sizeof(st), cudaMemcpyDeviceToHost));
+    memset(out, 0, sizeof(*out));
+    out->states = st.count;
+    out->min_state = st.gimin;
+    out->min_height = st.gfmin;
+    out->min_x = st.gxmin;
+    out->interval = st.interval;
+    out->searching = st.hsearch;
+    out->ev_found = !st.efield;
+    out->last_x = st.last_x;
+    out->last_height = st.last_f;
+    // the tool's summary line (tt_analysis.cc:169-171)
+    const double gtmin = st.gimin * st.interval;
+    out->t_rel = gtmin - S->prm.h0 / S->prm.V;
+    out->t_rel_ev = gtmin - st.tmin0_ev;
+    out->percent = st.count > 1 ? 100. * float(st.gimin) / float(st.count - 1) : 0.;
+    long n = std::min(cap, std::min(st.count, S->lcap));
+    if (n > 0) {
+        std::vector<double2> hb(n);
+        VDI_CUDA(cudaMemcpy(hb.data(), S->d_lhist, n * sizeof(double2), cudaMemcpyDeviceToHost));
+        for (long k = 0; k < n; k++) {
+            h_xmin[k] = hb[k].x;
+            h_fmin[k] = hb[k].y;
+        }
+    }
     return VDI_OK;
 }
 
@@ -613,8 +698,12 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     // MAC correction, two boundary kernels, the FEM source, the velocity update
     // and the final boundary kernel (+1 viscous source when implicit), two
     // kernels per initial guess; per solve two set-up kernels and the first
-    // residual check; per solve-loop iteration the kernels of its V-cycle.
-    long launches = S->steps * (11 + (S->prm.implicit_visc ? 1 : 0));
+    // residual check; per solve-loop iteration the kernels of its V-cycle;
+    // per step the lift-off search when it is on, and with the learned guess
+    // the residual kernel and the network's correction.
+    long per_step = 11 + (S->prm.implicit_visc ? 1 : 0) + (S->lcfg.mode != VDI_LIFTOFF_OFF ? 1 : 0) +
+                    (S->prm.mg_guess == VDI_GUESS_LEARNED ? 1 + unet_kernels_per_correction() : 0);
+    long launches = S->steps * per_step;
     for (int k = 0; k < 4; k++) {
         if (!S->mg[k]) continue;
         launches += out->solves[k] * (2 + 3) + out->vcycles[k] * mg_kernels_per_iteration(S->mg[k], S->prm.mg_precision);

@@ -760,6 +760,10 @@ int unet_correct(vdi_unet* u, cudaStream_t s, const double* r, const double* d_r
     return VDI_OK;
 }
 
+int unet_kernels_per_correction() {
+    return 4 + unet::NL;   // restrict, pack, one per layer, unpack, prolong
+}
+
 int unet_dims(const vdi_unet* u, int* H, int* W) {
     *H = u->net->H;
     *W = u->net->W;

@@ -128,6 +128,8 @@ int mg_residual_async(MG* mg, cudaStream_t s, const double* b, const double* z, 
  * scale * rms * (prolonged output) to z. in_buf/out_buf hold H x W floats. */
 int unet_correct(vdi_unet* u, cudaStream_t s, const double* r, const double* d_rnorm, double* z, int m, int n,
                  int factor, double scale, float* in_buf, float* out_buf);
+/** Kernels one unet_correct call launches. */
+int unet_kernels_per_correction();
 int unet_dims(const vdi_unet* u, int* H, int* W);
 
 }  // namespace vdi
