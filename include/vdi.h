@@ -87,6 +87,19 @@ enum vdi_mg_guess {
  * into *out with the default numerical options. */
 int vdi_params_from_cfg(const char* cfg_text, vdi_params* out);
 
+/* Run and output options of a .cfg text (fileinfo.cc:56-122): the output
+ * flags (fflags bits of the 'output' keyword), restart frequency, tracer count
+ * and machine-readable timing flag. Keywords outside the GPU path
+ * (gas_layer_data, nif_center, nif_range) return VDI_ERR_CONFIG. */
+typedef struct vdi_run_options {
+    unsigned int fflags;      /* 1 u, 2 v, 4 p, 8 pb, 16 pbfull, 32 w, 64 h, 128 fbd,
+                                 256 pg, 512 hfull, 1024 fbdfull, 2048 pgfull */
+    int restart_freq;         /* frames between restart files (0: none) */
+    int ntrace;               /* tracers (fileinfo.hh:26) */
+    int mr_time_output;       /* machine-readable timing lines */
+} vdi_run_options;
+int vdi_run_options_from_cfg(const char* cfg_text, vdi_run_options* out);
+
 /* --------------------------------------------------------- simulation */
 typedef struct vdi_sim vdi_sim;
 

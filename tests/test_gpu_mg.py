@@ -185,3 +185,85 @@ def test_matches_reference_dipole_solve(V, ref_driver, tmp_path):
         s.b.copy_(torch.from_numpy(b))
         s.solve_v_cycle(rtol=1e-13)
         assert _rel(s.z.cpu().numpy(), zr) < 1e-9, kind
+
+
+# ----------------------------------------------------------------- any size
+# Sizes the constant-stencil hierarchy cannot coarsen to a small level (an
+# odd factor in a side) run on the Galerkin hierarchy; VDI_MG_GENERAL=1 forces
+# it on power-of-two sizes too.
+
+@pytest.fixture
+def force_general(monkeypatch):
+    monkeypatch.setenv("VDI_MG_GENERAL", "1")
+
+
+@pytest.mark.parametrize("m,n", [(96, 64), (200, 100), (135, 77), (256, 128)])
+def test_mac_solve_any_size(V, m, n, monkeypatch):
+    torch = _torch()
+    if (m, n) == (256, 128):
+        monkeypatch.setenv("VDI_MG_GENERAL", "1")
+    dx, dy = 2. / (m - 1), 2. / (n - 1)
+    b = gaussians_rhs(m, n, seed=3)
+    A = vo.mac_matrix(m, n, 1. / (dx * dx), 1. / (dy * dy))
+    s = V.MgsMac(m, n, dx, dy)
+    s.b.copy_(torch.from_numpy(b))
+    v, rel = s.solve_v_cycle(rtol=1e-10)
+    z = s.z.cpu().numpy()
+    assert np.linalg.norm(b - A @ z) / np.linalg.norm(b) <= 1e-10 * (1 + 1e-6)
+    assert v <= 30, v
+    assert _rel(z, vo.DirectSolver(A).solve(b)) < 1e-6
+
+
+@pytest.mark.parametrize("M,N", [(96, 64), (201, 101), (57, 130), (257, 129)])
+def test_fem_solve_any_size(V, M, N, monkeypatch):
+    torch = _torch()
+    if (M, N) == (257, 129):
+        monkeypatch.setenv("VDI_MG_GENERAL", "1")
+    dx, dy = 1. / (M - 1), 1.2 / (N - 1)
+    rng = np.random.default_rng(17)
+    b = np.zeros((N, M))
+    b[1:, :] = rng.standard_normal((N - 1, M)) * dx * dy
+    c = vo.fem_coeffs(dx, dy)
+    b[0, :] = vo.fem_a_cc(M, N, np.arange(M), 0, c['fm']) * rng.uniform(1, 2, M)
+    b = b.ravel()
+    A = vo.fem_matrix(M, N, dx, dy)
+    s = V.MgsFem(M, N, dx, dy)
+    s.b.copy_(torch.from_numpy(b))
+    v, rel = s.solve_v_cycle(rtol=1e-10)
+    z = s.z.cpu().numpy()
+    assert np.linalg.norm(b - A @ z) / np.linalg.norm(b) <= 1e-10 * (1 + 1e-6)
+    assert v <= 30, v
+    assert _rel(z, vo.DirectSolver(A).solve(b)) < 1e-7
+
+
+@pytest.mark.parametrize("x_sym,horiz", [(True, True), (False, False)])
+@pytest.mark.parametrize("vf", [0.4, 40.0])
+def test_visc_solve_any_size(V, x_sym, horiz, vf):
+    torch = _torch()
+    m, n = 200, 100
+    b = np.random.default_rng(19).standard_normal(m * n)
+    A = vo.visco_matrix(m, n, vf, vf, x_sym, horiz)
+    s = V.ViscoImpl(m, n, x_sym, horiz, vf, vf)
+    s.b.copy_(torch.from_numpy(b))
+    v, rel = s.solve_v_cycle(rtol=1e-10)
+    z = s.z.cpu().numpy()
+    assert np.linalg.norm(b - A @ z) / np.linalg.norm(b) <= 1e-10 * (1 + 1e-6)
+    assert v <= 30, v
+    assert _rel(z, vo.DirectSolver(A).solve(b)) < 1e-9
+
+
+def test_general_vcycle_count_comparable(V, monkeypatch):
+    """On a power-of-two grid the general hierarchy converges in about as many
+    V-cycles as the constant-stencil one."""
+    torch = _torch()
+    m, n = 256, 128
+    dx = 1. / m
+    b = torch.from_numpy(gaussians_rhs(m, n, seed=9))
+    s = V.MgsMac(m, n, dx, dx)
+    s.b.copy_(b)
+    v_fast, _ = s.solve_v_cycle(rtol=1e-10)
+    monkeypatch.setenv("VDI_MG_GENERAL", "1")
+    g = V.MgsMac(m, n, dx, dx)
+    g.b.copy_(b)
+    v_gen, _ = g.solve_v_cycle(rtol=1e-10)
+    assert v_gen <= v_fast + 4, (v_gen, v_fast)

@@ -65,9 +65,40 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    _build_host()
     if verbose:
         print(LIB)
     return LIB
+
+
+HOST = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(OUT_DIR, "libvdi_host.so")
+HOST_CLI = os.path.join(OUT_DIR, "vdi_fluid_test")
+CUDA_HOME = os.path.dirname(os.path.dirname(NVCC))
+HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I", os.path.join(ROOT, "include"),
+              "-I", os.path.join(HOST, "include"), "-I", os.path.join(CUDA_HOME, "include")]
+
+
+def _build_host():
+    """The C++ drop-in classes (host/include, host/src) as libvdi_host.so over
+    libvdi.so, and the vdi_fluid_test driver."""
+    srcs = sorted(os.path.join(HOST, "src", f) for f in os.listdir(os.path.join(HOST, "src")) if f.endswith(".cc"))
+    hdrs = [os.path.join(HOST, "include", f) for f in os.listdir(os.path.join(HOST, "include"))]
+    deps = srcs + hdrs + [LIB, os.path.join(ROOT, "include", "vdi.h"), os.path.join(HOST, "vdi_fluid_test.cc")]
+    newest = max(os.path.getmtime(p) for p in deps)
+    if os.path.exists(HOST_CLI) and os.path.getmtime(HOST_CLI) >= newest and os.path.getmtime(HOST_LIB) >= newest:
+        return
+    link = ["-L", OUT_DIR, "-lvdi", "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart_static", "-ldl", "-lpthread",
+            "-lrt", "-Wl,-rpath,$ORIGIN"]
+    cmd = ["g++"] + HOST_FLAGS + ["-shared", "-o", HOST_LIB] + srcs + link
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host library build failed:\n{r.stdout}\n{r.stderr}")
+    cmd = ["g++"] + HOST_FLAGS + ["-o", HOST_CLI, os.path.join(HOST, "vdi_fluid_test.cc"), "-L", OUT_DIR,
+                                  "-lvdi_host", "-lvdi", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"vdi_fluid_test build failed:\n{r.stdout}\n{r.stderr}")
 
 
 if __name__ == "__main__":

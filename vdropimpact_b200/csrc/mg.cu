@@ -1109,6 +1109,8 @@ static cudaError_t cc_tile_attr() {
     return cudaFuncSetAttribute(cc_tile<T, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
 }
 
+#include "mg_general.cuh"
+
 class MG {
   public:
     int kind = 0;
@@ -1127,6 +1129,10 @@ class MG {
     std::vector<float*> z32, b32, t32;   // t: scratch iterate of each tiled level
     Reduce rd;
     SolveCtl* ctl = nullptr;
+    // grids the constant-stencil hierarchy cannot coarsen use the Galerkin
+    // hierarchy of mg_general.cuh (FP64 only)
+    bool general = false;
+    GenMG gen;
     int nu1 = 2, nu2 = 2;
     double rtol = 1e-10;
     int max_it = 200;
@@ -1144,6 +1150,7 @@ class MG {
         reduce_free(rd);
         if (ctl) cudaFree(ctl);
         ctl = nullptr;
+        gen.release();
     }
 
     bool fem() const { return kind == VDI_MG_FEM; }
@@ -1218,7 +1225,34 @@ class MG {
         return c;
     }
 
+    /** Chooses the hierarchy: the constant-stencil one when it reaches a
+     * small coarsest level (or, for the viscous systems, one weakly coupled
+     * enough for smoothing alone), the general one otherwise or when
+     * VDI_MG_GENERAL is set. */
     int build_levels() {
+        general = false;
+        const char* e = getenv("VDI_MG_GENERAL");
+        int st = build_fast_levels();
+        bool need = (e && atoi(e) != 0) || st != VDI_OK;
+        if (!need) {
+            const LevelD& C = lv.back();
+            bool small = size(nlev - 1) <= 64;
+            bool weak = kind != VDI_MG_MAC && kind != VDI_MG_FEM && 2 * (std::fabs(C.ox) + std::fabs(C.oy)) < 0.25;
+            need = !small && !weak;
+        }
+        if (!need) return VDI_OK;
+        lv.resize(1);
+        if (fem()) fill_fem(lv[0]);
+        else fill_cc(lv[0], c1, c2);
+        nlev = 1;
+        nmulti64 = nmulti32 = 0;
+        smooth_tail = false;
+        smem64 = smem32 = 0;
+        general = true;
+        return VDI_OK;
+    }
+
+    int build_fast_levels() {
         lv.clear();
         if (fem()) {
             double dydx = c2 / c1, dxdy = c1 / c2;
@@ -1290,6 +1324,22 @@ class MG {
     }
 
     int alloc() {
+        if (general) {
+            VDI_TRY(reduce_alloc(rd, MAX_PARTIALS));
+            VDI_CUDA(cudaMalloc(&ctl, sizeof(SolveCtl)));
+            VDI_CUDA(cudaMemset(ctl, 0, sizeof(SolveCtl)));
+            VDI_TRY(set_ctl_params(0, rtol, max_it));
+            const long N0 = size(0);
+            auto apply = [&](const double* z, double* y) -> int {
+                if (fem()) apply_k<double><<<nblk(N0), 256>>>(femc<double>(0), z, y);
+                else apply_k<double><<<nblk(N0), 256>>>(ccc<double>(0), z, y);
+                VDI_CUDA(cudaGetLastError());
+                return VDI_OK;
+            };
+            VDI_TRY(gen.setup(m, n, apply));
+            VDI_CUDA(cudaDeviceSynchronize());
+            return VDI_OK;
+        }
         z64.assign(nlev, nullptr); b64.assign(nlev, nullptr);
         z32.assign(nlev, nullptr); b32.assign(nlev, nullptr);
         t64.assign(nlev, nullptr); t32.assign(nlev, nullptr);
@@ -1415,6 +1465,11 @@ class MG {
     }
 
     int vcycle64(cudaStream_t s, const double* b, double* z, int norm, int use_cond, cudaGraphConditionalHandle h) {
+        if (general) {
+            VDI_TRY(gen.vcycle(s, 0, b, z));
+            if (norm) VDI_TRY(enqueue_resid_norm(s, b, z, 1, use_cond, h));
+            return VDI_OK;
+        }
         VDI_TRY(vcycle<double>(s, 0, b, z, nmulti64, z64, b64, smem64, 0, norm && nmulti64 > 0, use_cond, h));
         if (norm && nmulti64 == 0) VDI_TRY(enqueue_resid_norm(s, b, z, 1, use_cond, h));
         return VDI_OK;
@@ -1426,7 +1481,9 @@ class MG {
     int enqueue_resid_norm(cudaStream_t s, const double* b, const double* z, int count_cycle, int use_cond,
                            cudaGraphConditionalHandle h) {
         int nb = rblocks(size(0));
-        if (fem())
+        if (general)
+            resid_norm_k<double><<<nb, 256, 0, s>>>(gen.op(0), z, b, rd, ctl, count_cycle, use_cond, h);
+        else if (fem())
             resid_norm_k<double><<<nb, 256, 0, s>>>(femc<double>(0), z, b, rd, ctl, count_cycle, use_cond, h);
         else
             resid_norm_k<double><<<nb, 256, 0, s>>>(ccc<double>(0), z, b, rd, ctl, count_cycle, use_cond, h);
@@ -1457,7 +1514,7 @@ class MG {
      * the residual norm of the new iterate and the solve decision. */
     int enqueue_body(cudaStream_t s, const double* b, double* z, int precision, int use_cond,
                      cudaGraphConditionalHandle h) {
-        if (precision == VDI_MG_MIXED) {
+        if (precision == VDI_MG_MIXED && !general) {
             VDI_TRY(vcycle32(s));
             add_f32_to_f64<<<nblk(size(0)), 256, 0, s>>>(z, z32[0], size(0));
             VDI_TRY(enqueue_resid32(s, b, z, 1, use_cond, h));
@@ -1469,7 +1526,7 @@ class MG {
 
     int enqueue_first_check(cudaStream_t s, const double* b, const double* z, int precision, int use_cond,
                             cudaGraphConditionalHandle h) {
-        if (precision == VDI_MG_MIXED) return enqueue_resid32(s, b, z, 0, use_cond, h);
+        if (precision == VDI_MG_MIXED && !general) return enqueue_resid32(s, b, z, 0, use_cond, h);
         return enqueue_resid_norm(s, b, z, 0, use_cond, h);
     }
 
@@ -1623,6 +1680,7 @@ int mg_residual(MG* mg, cudaStream_t s, const double* b, const double* z, double
 }
 
 int mg_kernels_per_iteration(const MG* mg, int precision) {
+    if (mg->general) return mg->gen.kernels_per_vcycle() + 1;
     int nm = precision == VDI_MG_MIXED ? mg->nmulti32 : mg->nmulti64;
     int k = 2 * nm + 1;                       // PRE/POST per tiled level + the coarsest
     if (precision == VDI_MG_MIXED) k += 2;    // FP64 update and residual
@@ -1755,6 +1813,10 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
     MG* g = new MG();
     g->kind = k.kind; g->m = k.m; g->n = k.n; g->c1 = k.c1; g->c2 = k.c2; g->x_sym = k.x_sym;
     int st = g->build_levels();
+    if (st == VDI_OK && g->general) {
+        set_error("vdi_mg_solve_noalloc: a %dx%d grid needs the general hierarchy, which allocates", k.m, k.n);
+        st = VDI_ERR_UNSUPPORTED_SIZE;
+    }
     if (st != VDI_OK) {
         delete g;
         return st;

@@ -308,9 +308,65 @@ int parse_cfg(const char* text, vdi_params* P) {
     return VDI_OK;
 }
 
+int parse_run_options(const char* text, vdi_run_options* O) {
+    // fileinfo.cc:56-122: the keywords that control the run and its output
+    memset(O, 0, sizeof(*O));
+    std::istringstream in(text);
+    std::string line;
+    int ln = 0;
+    while (std::getline(in, line)) {
+        ln++;
+        size_t h = line.find('#');
+        if (h != std::string::npos) line = line.substr(0, h);
+        std::istringstream ls(line);
+        std::string key, t;
+        if (!(ls >> key)) continue;
+        std::vector<std::string> vals;
+        while (ls >> t) vals.push_back(t);
+        if (key == "restart_freq" || key == "tracers") {
+            if (vals.size() != 1) {
+                set_error("%s needs one value (line %d)", key.c_str(), ln);
+                return VDI_ERR_CONFIG;
+            }
+            (key == "tracers" ? O->ntrace : O->restart_freq) = atoi(vals[0].c_str());
+        } else if (key == "mr_time_output") {
+            O->mr_time_output = 1;
+        } else if (key == "output") {
+            static const char* names[] = {"u", "v", "p", "pb", "pbfull", "w", "h", "fbd", "pg", "hfull",
+                                          "fbdfull", "pgfull"};
+            O->fflags = 0;
+            for (auto& v : vals) {
+                int k = 0;
+                while (k < 12 && v != names[k]) k++;
+                if (k == 12) {
+                    set_error("Output type not understood (line %d)", ln);
+                    return VDI_ERR_CONFIG;
+                }
+                O->fflags |= 1u << k;
+            }
+        } else if (key == "gas_layer_data" || key == "nif_center" || key == "nif_range") {
+            set_error("option '%s' is outside the GPU path (line %d)", key.c_str(), ln);
+            return VDI_ERR_CONFIG;
+        }
+    }
+    if (O->restart_freq < 0 || O->ntrace < 0) {
+        set_error("Value of restart_freq or tracers invalid");
+        return VDI_ERR_CONFIG;
+    }
+    return VDI_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int vdi_run_options_from_cfg(const char* text, vdi_run_options* out) {
+    if (!text || !out) return VDI_ERR_INVALID_ARGUMENT;
+    vdi_params P;
+    int st = parse_cfg(text, &P);
+    if (st != VDI_OK) return st;
+    return parse_run_options(text, out);
+}
 
 const char* vdi_status_string(int s) {
     switch (s) {

@@ -1,0 +1,83 @@
+// The step driver with the public interface of the reference's fluid_2d
+// (fluid_2d.hh:21-142) over a B200 simulation (vdi_sim of include/vdi.h).
+//
+// step_forward, init_fields and solve run on the device; the frame output
+// (write_files and the Gnuplot formats of fluid_2d_sio.cc:140-224) and the
+// restart files (fluid_2d_sio.cc:39-119) are byte-compatible with the
+// reference's. fbase/fm hold host copies of u, v, p that sync_fields()
+// refreshes; the output and restart routines call it themselves. Tracers and
+// the non-inertial frame are outside the GPU path: a configuration that asks
+// for them stops with a fatal error.
+#ifndef VDI_HOST_FLUID_2D_HH
+#define VDI_HOST_FLUID_2D_HH
+
+#include <cstdio>
+
+#include "common.hh"
+#include "fields.hh"
+#include "fileinfo.hh"
+#include "vdi.h"
+
+class fluid_2d : public fileinfo {
+    public:
+        const int mn;
+        const int me;
+        const int ne;
+        const int ml;
+        const double dx;
+        const double dy;
+        const double xsp;
+        const double ysp;
+        const double xxsp;
+        const double yysp;
+        const double dt_reg;
+        /** Host copy of the primary fields over the ghosted grid. */
+        field* const fbase;
+        /** The (0,0) cell of fbase. */
+        field* const fm;
+        /** Tracer positions (none on the GPU path). */
+        double* const tm;
+        /** A host source array of the node grid (me*ne), the right-hand side
+         * that a standalone visco_impl bound to this object solves with. */
+        double* const src;
+        double time;
+        int f_num;
+        fluid_2d(const char* infile);
+        ~fluid_2d();
+        void solve();
+        void step_forward(double dt);
+        void init_fields();
+        void load_restart(int sn);
+        void load_last_restart();
+        void save_restart(int sn);
+        void write_files(int k);
+        void output(const char* prefix, const int mode, int sn, bool ghost = false);
+        void output_pbase_full(int sn);
+        inline int timestep_select(double interval, double& adt) {
+            int l = static_cast<int>(interval / dt_reg) + 1;
+            adt = interval / l;
+            return l;
+        }
+        inline FILE* odir_open(const char* prefix, int sn, const char* mode) {
+            char* bufc = reinterpret_cast<char*>(buf);
+            sprintf(bufc, "%s/%s.%d", filename, prefix, sn);
+            return safe_fopen(bufc, mode);
+        }
+        /** Copies u, v, p, the gas-layer arrays and the time from the device
+         * into fbase/fm, gl and time. */
+        void sync_fields();
+        /** The device simulation (for callers of the C ABI). */
+        vdi_sim* sim() { return S; }
+    private:
+        vdi_sim* S;
+        float* buf;
+        bool restart_exists(int sn);
+        /** Copies fbase/fm, gl and time to the device. */
+        void push_fields();
+        inline double vorticity(field* fp) {
+            return 0.5 * (xsp * (fp->v - fp[-1].v + fp[-ml].v - fp[-ml - 1].v) -
+                          ysp * (fp->u + fp[-1].u - fp[-ml].u - fp[-ml - 1].u));
+        }
+};
+
+#endif

@@ -1,0 +1,95 @@
+// Host side of the gas layer: restart records (gas_layer.hh:38-45,
+// gas_layer_solve.cc:313-331) and the profile outputs
+// (gas_layer_solve.cc:258-308), byte-compatible with the reference's.
+#include "gas_layer.hh"
+
+#include <cstring>
+
+#include "common.hh"
+
+gas_layer::gas_layer(int m_, double ax_, double bx_, double Vframe_)
+    : m(m_), me(m_ + 1), ml(m_ + 4), ax(ax_), bx(bx_), dx((bx_ - ax_) / m_), Vframe(Vframe_), p(new double[me]()),
+      tau(new double[ml]()), p_old(new double[me]()), tau_old(new double[ml]()) {}
+
+gas_layer::~gas_layer() {
+    delete[] tau_old;
+    delete[] p_old;
+    delete[] tau;
+    delete[] p;
+}
+
+void gas_layer::apply_tau_bc() {
+    tau[0] = -tau[3];
+    tau[1] = -tau[2];
+    tau[ml - 2] = -tau[ml - 3];
+    tau[ml - 1] = -tau[ml - 4];
+}
+
+void gas_layer::load_restart(double time, FILE* inf) {
+    safe_fread(&Vframe, sizeof(double), 1, inf, "Vframe");
+    load_restart_internal(time, inf);
+}
+
+void gas_layer::save_restart(FILE* outf) {
+    fwrite(&Vframe, sizeof(double), 1, outf);
+    save_restart_internal(outf);
+}
+
+gas_layer_solve::gas_layer_solve(int m_, double ax_, double bx_, double R_, double V_, double h0_)
+    : gas_layer(m_, ax_, bx_, V_), R(R_), V(V_), h0(h0_), h(new double[m_]()), ht(new double[m_]()),
+      fbd(new double[m_]()), pg(new double[m_ + 1]()) {}
+
+gas_layer_solve::~gas_layer_solve() {
+    delete[] pg;
+    delete[] fbd;
+    delete[] ht;
+    delete[] h;
+}
+
+void gas_layer_solve::load_restart_internal(double time, FILE* inf) {
+    safe_fread(p, sizeof(double), me, inf, "p array");
+    safe_fread(tau + 2, sizeof(double), m, inf, "tau array");
+    apply_tau_bc();
+    safe_fread(h, sizeof(double), m, inf, "h array");
+    safe_fread(ht, sizeof(double), m, inf, "ht array");
+    safe_fread(pg, sizeof(double), me, inf, "pg array");
+    // the boundary flux is not part of the record; the next update sets it
+    memset(fbd, 0, m * sizeof(double));
+}
+
+void gas_layer_solve::save_restart_internal(FILE* outf) {
+    fwrite(p, sizeof(double), me, outf);
+    fwrite(tau + 2, sizeof(double), m, outf);
+    fwrite(h, sizeof(double), m, outf);
+    fwrite(ht, sizeof(double), m, outf);
+    fwrite(pg, sizeof(double), me, outf);
+}
+
+void gas_layer_solve::output_profile(const char* filename, float* buf, int sn, double ay, int fld) {
+    char* bufc = reinterpret_cast<char*>(buf);
+    sprintf(bufc, fld == 0 ? "%s/height.%d" : (fld == 1 ? "%s/fbd.%d" : "%s/pg.%d"), filename, sn);
+    FILE* outf = safe_fopen(bufc, "wb");
+    int l = fld == 2 ? me : m;
+    float* bp = buf + 1;
+    *buf = l;
+    for (int i = 0; i < l; i++) *(bp++) = ax + (i + (fld == 2 ? 0 : 0.5)) * dx;
+    fwrite(buf, sizeof(float), l + 1, outf);
+    *buf = ay;
+    bp = buf + 1;
+    const double* hp = fld == 0 ? h : (fld == 1 ? fbd : pg);
+    for (int i = 0; i < l; i++) *(bp++) = hp[i];
+    fwrite(buf, sizeof(float), l + 1, outf);
+    fclose(outf);
+}
+
+void gas_layer_solve::output_profile_double(const char* filename, float* buf, int sn, int fld) {
+    char* bufc = reinterpret_cast<char*>(buf);
+    sprintf(bufc, fld == 0 ? "%s/hfull.%d" : (fld == 1 ? "%s/fbdfull.%d" : "%s/pgfull.%d"), filename, sn);
+    FILE* outf = safe_fopen(bufc, "wb");
+    int l = fld == 2 ? me : m;
+    fwrite(&l, sizeof(int), 1, outf);
+    fwrite(&ax, sizeof(double), 1, outf);
+    fwrite(&bx, sizeof(double), 1, outf);
+    fwrite(fld == 0 ? h : (fld == 1 ? fbd : pg), sizeof(double), l, outf);
+    fclose(outf);
+}
