@@ -156,6 +156,46 @@ int vdi_sim_stats(vdi_sim* sim, vdi_stats* out, int reset);
  * 6 the last MAC source, 7 the last MAC solution (m*n each). */
 int vdi_sim_device_field(vdi_sim* sim, int which, double** d_ptr, size_t* count);
 
+/* ----------------------------------------------------------- autotuning
+ * Picks, by timing on this GPU with the simulation's own arrays, the launch
+ * shape of the per-cell stencil kernels and, for each multigrid system, the
+ * level below which the single-CTA coarse cycle replaces the per-level tile
+ * kernels. Results are cached in the process per grid (m, n, x_sym,
+ * implicit_visc), so simulations of one grid tune once. Restarts the step
+ * graph. No reference counterpart (the reference has no tunable kernels). */
+typedef struct vdi_tune {
+    int blk_x, blk_y;         /* launch shape of the per-cell kernels */
+    long cta_limit[4];        /* per system (MAC, FEM, VX, VY): bytes below which
+                                 levels run in one CTA; 0 when absent */
+    int tiled_levels[4];      /* the resulting per-launch levels (-1: general hierarchy) */
+    float stencil_ms;         /* the four advection stages with the chosen shape */
+    float vcycle_ms[4];       /* one FP64 V-cycle per system with the chosen cut */
+    int from_cache;           /* 1 when an earlier tuning of the same grid was reused */
+} vdi_tune;
+int vdi_sim_autotune(vdi_sim* sim, vdi_tune* out);
+/* Applies a tuning (for example one saved from an earlier process). */
+int vdi_sim_set_tuning(vdi_sim* sim, const vdi_tune* tune);
+
+/* ---------------------------------------------------------------- batch
+ * Independent simulations (a viscosity or impact-velocity sweep over uneven
+ * grids) stepped together: one timestep of the batch is one CUDA graph with a
+ * branch per simulation, launched once. Each simulation keeps its own arrays
+ * and is reachable through vdi_batch_sim for state, statistics and lift-off. No reference
+ * counterpart (the reference runs one configuration per process). */
+typedef struct vdi_batch vdi_batch;
+int vdi_batch_create(const vdi_params* prms, int count, vdi_batch** out);
+int vdi_batch_destroy(vdi_batch* batch);
+int vdi_batch_size(const vdi_batch* batch);
+int vdi_batch_sim(vdi_batch* batch, int k, vdi_sim** out);
+int vdi_batch_init_fields(vdi_batch* batch);
+/* Autotunes every simulation (grids tune once); out may be NULL or hold
+ * count entries. */
+int vdi_batch_autotune(vdi_batch* batch, vdi_tune* out);
+/* nsteps timesteps of every simulation, simulation k with step dts[k]. The
+ * first call with a new set of steps captures the graph. Returns the first
+ * simulation's error, naming its index. */
+int vdi_batch_step_forward(vdi_batch* batch, const double* dts, int nsteps);
+
 /* ------------------------------------------------------ lift-off search
  * The reference's analysis tool (tt_analysis.cc:97-171) run on the device
  * after every step: the minimum of the gas-layer height profile (as the

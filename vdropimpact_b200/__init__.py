@@ -74,7 +74,23 @@ class Fluid2D:
             self.use_graph(True)
 
     # ------------------------------------------------------------------
+    @classmethod
+    def _view(cls, handle, prm, owner):
+        """A simulation owned by a Batch (not destroyed by this object)."""
+        f = cls.__new__(cls)
+        f.prm = prm
+        f.m, f.n = prm.m, prm.n
+        f.me, f.ne, f.ml = f.m + 1, f.n + 1, f.m + 4
+        f.dx = (prm.bx - prm.ax) / f.m
+        f.dy = (prm.by - prm.ay) / f.n
+        f._h = handle
+        f._owner = owner
+        return f
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             lib().vdi_sim_destroy(self._h)
             self._h = None
@@ -175,6 +191,14 @@ class Fluid2D:
                     height_fixed_point_iters=s.height_fixed_point_iters,
                     last_rel_res=dict(zip(names, list(s.last_rel_res))), kernel_launches=s.kernel_launches)
 
+    def autotune(self) -> dict:
+        """Times the candidate launch shapes of the stencil kernels and the
+        tile/CTA cut of each multigrid hierarchy on this grid, and keeps the
+        fastest (cached per grid in the process)."""
+        t = _abi.VdiTune()
+        check(lib().vdi_sim_autotune(self._h, C.byref(t)), "vdi_sim_autotune")
+        return _tune_dict(t)
+
     LIFTOFF = {"off": 0, "smoothed": 1, "raw": 2}
 
     def liftoff_setup(self, mode="smoothed", every: int = 1, history: int = 0):
@@ -209,6 +233,88 @@ class Fluid2D:
         n = C.c_size_t()
         check(lib().vdi_sim_device_field(self._h, which, C.byref(p), C.byref(n)), "vdi_sim_device_field")
         return C.cast(p, C.c_void_p).value, n.value
+
+
+def _tune_dict(t) -> dict:
+    return dict(block=(t.blk_x, t.blk_y), cta_limit=list(t.cta_limit), tiled_levels=list(t.tiled_levels),
+                stencil_ms=t.stencil_ms, vcycle_ms=list(t.vcycle_ms), from_cache=bool(t.from_cache))
+
+
+class Batch:
+    """Independent simulations stepped together, one CUDA graph (a branch
+    per simulation) per timestep. cfgs: .cfg texts or VdiParams."""
+
+    def __init__(self, cfgs, *, mg_rtol: float = 1e-10, mg_max_vcycles: int = 200, mg_precision="fp64",
+                 mg_guess="linear"):
+        prms = []
+        for c in cfgs:
+            p = c if isinstance(c, _abi.VdiParams) else params_from_cfg(c)
+            p.mg_rtol = mg_rtol
+            p.mg_max_vcycles = mg_max_vcycles
+            p.mg_precision = _PREC[mg_precision]
+            p.mg_guess = Fluid2D.GUESS[mg_guess] if isinstance(mg_guess, str) else int(mg_guess)
+            prms.append(p)
+        arr = (_abi.VdiParams * len(prms))(*prms)
+        h = C.c_void_p()
+        check(lib().vdi_batch_create(arr, len(prms), C.byref(h)), "vdi_batch_create")
+        self._h = h
+        self.sims = []
+        for k, p in enumerate(prms):
+            sh = C.c_void_p()
+            check(lib().vdi_batch_sim(h, k, C.byref(sh)), "vdi_batch_sim")
+            self.sims.append(Fluid2D._view(sh, p, self))
+
+    def __len__(self):
+        return len(self.sims)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for s in self.sims:
+                s._h = None
+            lib().vdi_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_fields(self):
+        check(lib().vdi_batch_init_fields(self._h), "vdi_batch_init_fields")
+
+    def frame_dts(self):
+        return [s.frame_dt() for s in self.sims]
+
+    def autotune(self):
+        out = (_abi.VdiTune * len(self.sims))()
+        check(lib().vdi_batch_autotune(self._h, out), "vdi_batch_autotune")
+        return [_tune_dict(t) for t in out]
+
+    def step_forward(self, dts, nsteps: int = 1):
+        arr = (C.c_double * len(self.sims))(*[float(d) for d in dts])
+        check(lib().vdi_batch_step_forward(self._h, arr, nsteps), "vdi_batch_step_forward")
+
+
+def sweep_configs(count: int, seed: int = 0, sizes=(256, 512, 1024)):
+    """A seeded viscosity / impact-velocity sweep in the manner of the
+    reference's sims/create_cfg.pl: viscosity log-uniform in 1-100 cSt, impact
+    velocity uniform in 0.2-0.5 m/s, grid m x m/2 with m drawn from sizes; the
+    larger domain (L_nd 45, t_end_nd 100) from 25 cSt up, as create_cfg.pl
+    switches it. Returns .cfg texts."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nu = float(np.exp(rng.uniform(np.log(1.0), np.log(100.0))))
+        V = float(rng.uniform(0.2, 0.5))
+        m = int(rng.choice(sizes))
+        big = nu >= 25
+        out.append("\n".join([
+            f"grid_points {m} {m // 2}", f"L_nd {45 if big else 30}", "h0_nd 15",
+            f"t_end_nd {100 if big else 50}", "frames 250", "tmult 8e-3", f"nul_cSt {nu:.6g}", "rhol 997.96",
+            "R 1.5e-3", f"V {V:.6g}", "gamma 1.4", "sigma 72e-3", "mug 1.820775e-5", "Pamb 1e5", "x_sym",
+            "implicit_visc", "gas_layer_model"]) + "\n")
+    return out
 
 
 def profile_min(h, ax: float, dx: float, mode: str = "smoothed"):

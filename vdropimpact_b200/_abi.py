@@ -78,6 +78,11 @@ class VdiLiftoff(C.Structure):
                 ("last_height", C.c_double)]
 
 
+class VdiTune(C.Structure):
+    _fields_ = [("blk_x", C.c_int), ("blk_y", C.c_int), ("cta_limit", C.c_long * 4), ("tiled_levels", C.c_int * 4),
+                ("stencil_ms", C.c_float), ("vcycle_ms", C.c_float * 4), ("from_cache", C.c_int)]
+
+
 class VdiError(RuntimeError):
     def __init__(self, status: int, where: str, detail: str):
         super().__init__(f"{where}: status {status} ({_status_string(status)}): {detail}")
@@ -111,6 +116,15 @@ _SIGS = [
     ("vdi_sim_set_state", C.c_int, [C.c_void_p, C.POINTER(VdiState)]),
     ("vdi_sim_stats", C.c_int, [C.c_void_p, C.POINTER(VdiStats), C.c_int]),
     ("vdi_sim_device_field", C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(C.c_size_t)]),
+    ("vdi_sim_autotune", C.c_int, [C.c_void_p, C.POINTER(VdiTune)]),
+    ("vdi_sim_set_tuning", C.c_int, [C.c_void_p, C.POINTER(VdiTune)]),
+    ("vdi_batch_create", C.c_int, [C.POINTER(VdiParams), C.c_int, C.POINTER(C.c_void_p)]),
+    ("vdi_batch_destroy", C.c_int, [C.c_void_p]),
+    ("vdi_batch_size", C.c_int, [C.c_void_p]),
+    ("vdi_batch_sim", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    ("vdi_batch_init_fields", C.c_int, [C.c_void_p]),
+    ("vdi_batch_autotune", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("vdi_batch_step_forward", C.c_int, [C.c_void_p, _dp, C.c_int]),
     ("vdi_sim_liftoff_setup", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_long]),
     ("vdi_sim_liftoff", C.c_int, [C.c_void_p, C.POINTER(VdiLiftoff), C.c_void_p, C.c_void_p, C.c_long]),
     ("vdi_profile_min", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p, _dp, _dp]),

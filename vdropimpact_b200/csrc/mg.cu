@@ -1133,6 +1133,9 @@ class MG {
     // hierarchy of mg_general.cuh (FP64 only)
     bool general = false;
     GenMG gen;
+    // levels whose arrays fit in this many bytes run in the single-CTA cycle
+    // (autotuned per grid; at most CTA_SMEM_LIMIT)
+    size_t cta_limit = CTA_SMEM_LIMIT;
     int nu1 = 2, nu2 = 2;
     double rtol = 1e-10;
     int max_it = 200;
@@ -1310,10 +1313,10 @@ class MG {
         };
         nmulti64 = -1;
         for (int l = 0; l < nlev; l++)
-            if (tail_bytes(l, 8) <= CTA_SMEM_LIMIT) { nmulti64 = l; break; }
+            if (tail_bytes(l, 8) <= cta_limit) { nmulti64 = l; break; }
         nmulti32 = -1;
         for (int l = 0; l < nlev; l++)
-            if (tail_bytes(l, 4) <= CTA_SMEM_LIMIT) { nmulti32 = l; break; }
+            if (tail_bytes(l, 4) <= cta_limit) { nmulti32 = l; break; }
         if (nmulti64 < 0 || nmulti32 < 0) {
             set_error("multigrid: %dx%d grid does not coarsen to a shared-memory-sized level", m, n);
             return VDI_ERR_UNSUPPORTED_SIZE;
@@ -1580,6 +1583,25 @@ int mg_set_visc(MG* mg, double vfx, double vfy) {
     mg->max_it = mx;
     VDI_TRY(mg->build_levels());
     return mg->alloc();
+}
+
+int mg_set_cta_limit(MG* mg, size_t bytes) {
+    if (bytes < 1024 || bytes > CTA_SMEM_LIMIT) return VDI_ERR_INVALID_ARGUMENT;
+    if (bytes == mg->cta_limit) return VDI_OK;
+    double rt = mg->rtol;
+    int mx = mg->max_it;
+    mg->release();
+    mg->cta_limit = bytes;
+    mg->rtol = rt;
+    mg->max_it = mx;
+    VDI_TRY(mg->build_levels());
+    return mg->alloc();
+}
+
+size_t mg_cta_limit(const MG* mg) { return mg->cta_limit; }
+int mg_tiled_levels(const MG* mg, int precision) {
+    if (mg->general) return -1;
+    return precision == VDI_MG_MIXED ? mg->nmulti32 : mg->nmulti64;
 }
 
 SolveCtl* mg_ctl(MG* mg) { return mg->ctl; }

@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -405,6 +407,7 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     Grid& g = S->g;
     const vdi_params& P = S->prm;
     g.m = P.m; g.n = P.n; g.x_sym = P.x_sym; g.implicit_visc = P.implicit_visc;
+    g.blk_x = 32; g.blk_y = 8;
     g.ax = P.ax; g.ay = P.ay; g.bx = P.bx; g.by = P.by;
     // fluid_2d.cc:15-17
     g.dx = (P.bx - P.ax) / P.m;
@@ -886,3 +889,309 @@ int vdi_tri_solve(int n, double* d_a, double* d_b, double* d_c, double* d_d, voi
 }
 
 }  // extern "C"
+
+// ============================================================ autotuning
+// The per-cell stencil kernels take their launch shape from the Grid, and
+// each multigrid hierarchy switches from per-level tile kernels to the
+// single-CTA coarse cycle below a byte threshold. Both are chosen here by
+// timing the candidates with CUDA events on the simulation's own arrays; a
+// process-wide cache keyed by the grid lets simulations of the same grid
+// reuse a tuning.
+namespace {
+
+struct TuneKey {
+    int m, n, x_sym, iv;
+    bool operator<(const TuneKey& o) const {
+        if (m != o.m) return m < o.m;
+        if (n != o.n) return n < o.n;
+        if (x_sym != o.x_sym) return x_sym < o.x_sym;
+        return iv < o.iv;
+    }
+};
+
+std::map<TuneKey, vdi_tune>& tune_cache() {
+    static std::map<TuneKey, vdi_tune> c;
+    return c;
+}
+std::mutex& tune_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+
+const int BLOCK_SHAPES[][2] = {{32, 8}, {64, 4}, {128, 2}, {32, 4}, {64, 2}, {32, 16}, {64, 8}, {128, 4}, {256, 1}};
+const size_t CTA_LIMITS[] = {200 * 1024, 96 * 1024, 48 * 1024, 24 * 1024, 12 * 1024, 6 * 1024};
+
+/** Mean time of the four advection stages (idempotent as a group: each
+ * repetition recomputes from u, v, p). */
+int time_stencils(vdi_sim* S, double dt, float* ms) {
+    cudaEvent_t e0, e1;
+    VDI_CUDA(cudaEventCreate(&e0));
+    VDI_CUDA(cudaEventCreate(&e1));
+    auto run = [&]() -> int {
+        VDI_TRY(launch_stage1(S->s, S->g, S->f, dt));
+        VDI_TRY(launch_stage2(S->s, S->g, S->f));
+        VDI_TRY(launch_stage34(S->s, S->g, S->f, dt));
+        VDI_TRY(launch_stage5_src(S->s, S->g, S->f, S->gas, dt, S->src_mac));
+        return VDI_OK;
+    };
+    int st = VDI_OK;
+    for (int r = 0; r < 2 && st == VDI_OK; r++) st = run();
+    cudaEventRecord(e0, S->s);
+    for (int r = 0; r < 10 && st == VDI_OK; r++) st = run();
+    cudaEventRecord(e1, S->s);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (st == VDI_OK && e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    VDI_TRY(st);
+    VDI_CUDA(e);
+    *ms /= 10;
+    return VDI_OK;
+}
+
+/** Mean time of one FP64 V-cycle of system k on scratch arrays. */
+int time_vcycle(vdi_sim* S, int k, const double* src, float* ms) {
+    MG* g = S->mg[k];
+    size_t n = size_t(mg_fine_size(g));
+    double *b = nullptr, *z = nullptr;
+    VDI_CUDA(cudaMalloc(&b, n * 8));
+    VDI_CUDA(cudaMalloc(&z, n * 8));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = VDI_OK;
+    cudaError_t e = cudaMemcpyAsync(b, src, n * 8, cudaMemcpyDeviceToDevice, S->s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(z, 0, n * 8, S->s);
+    for (int r = 0; r < 2 && st == VDI_OK && e == cudaSuccess; r++) st = mg_v_cycle(g, S->s, b, z);
+    cudaEventRecord(e0, S->s);
+    for (int r = 0; r < 8 && st == VDI_OK && e == cudaSuccess; r++) st = mg_v_cycle(g, S->s, b, z);
+    cudaEventRecord(e1, S->s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (st == VDI_OK && e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(b);
+    cudaFree(z);
+    VDI_TRY(st);
+    VDI_CUDA(e);
+    *ms /= 8;
+    return VDI_OK;
+}
+
+const double* system_source(vdi_sim* S, int k) {
+    return k == SOLVER_MAC ? S->src_mac : k == SOLVER_FEM ? S->src_fem : k == SOLVER_VX ? S->su : S->sv;
+}
+
+int apply_tuning(vdi_sim* S, const vdi_tune& t) {
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    destroy_graph(S);
+    S->g.blk_x = t.blk_x;
+    S->g.blk_y = t.blk_y;
+    for (int k = 0; k < 4; k++)
+        if (S->mg[k] && t.cta_limit[k] > 0) VDI_TRY(mg_set_cta_limit(S->mg[k], size_t(t.cta_limit[k])));
+    return VDI_OK;
+}
+
+}  // namespace
+
+int vdi_sim_autotune(vdi_sim* S, vdi_tune* out) {
+    if (!S) return VDI_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    TuneKey key{S->prm.m, S->prm.n, S->prm.x_sym, S->prm.implicit_visc};
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) {
+        vdi_tune t = it->second;
+        t.from_cache = 1;
+        VDI_TRY(apply_tuning(S, t));
+        if (out) *out = t;
+        return VDI_OK;
+    }
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    destroy_graph(S);
+    // the frame timestep gives the viscous systems their hierarchy
+    double dt;
+    VDI_TRY(vdi_sim_timestep_select(S, S->prm.t_end / S->prm.nframes, &dt, nullptr));
+    VDI_TRY(update_visc(S, dt));
+    vdi_tune t{};
+    float best = 1e30f;
+    for (auto& b : BLOCK_SHAPES) {
+        S->g.blk_x = b[0];
+        S->g.blk_y = b[1];
+        float ms;
+        VDI_TRY(time_stencils(S, dt, &ms));
+        if (ms < best * 0.98f) {
+            best = ms;
+            t.blk_x = b[0];
+            t.blk_y = b[1];
+        }
+    }
+    S->g.blk_x = t.blk_x;
+    S->g.blk_y = t.blk_y;
+    t.stencil_ms = best;
+    for (int k = 0; k < 4; k++) {
+        MG* g = S->mg[k];
+        if (!g || mg_tiled_levels(g, VDI_MG_FP64) < 0) {
+            t.tiled_levels[k] = g ? -1 : 0;
+            continue;
+        }
+        float bk = 1e30f;
+        size_t bl = mg_cta_limit(g);
+        int seen = -2;
+        for (size_t lim : CTA_LIMITS) {
+            VDI_TRY(mg_set_cta_limit(g, lim));
+            int tl = mg_tiled_levels(g, VDI_MG_FP64);
+            if (tl == seen) continue;
+            seen = tl;
+            float ms;
+            VDI_TRY(time_vcycle(S, k, system_source(S, k), &ms));
+            if (ms < bk * 0.98f) {
+                bk = ms;
+                bl = lim;
+            }
+        }
+        VDI_TRY(mg_set_cta_limit(g, bl));
+        t.cta_limit[k] = long(bl);
+        t.tiled_levels[k] = mg_tiled_levels(g, VDI_MG_FP64);
+        t.vcycle_ms[k] = bk;
+    }
+    tune_cache()[key] = t;
+    if (out) *out = t;
+    return VDI_OK;
+}
+
+int vdi_sim_set_tuning(vdi_sim* S, const vdi_tune* t) {
+    if (!S || !t || t->blk_x < 1 || t->blk_y < 1 || t->blk_x * t->blk_y > 1024) return VDI_ERR_INVALID_ARGUMENT;
+    return apply_tuning(S, *t);
+}
+
+// ================================================================ batch
+// Independent simulations stepped together. Each keeps its own stream and
+// arrays; a timestep of the batch is one CUDA graph with one branch per
+// simulation (each branch the simulation's captured step, with its own
+// conditional multigrid loops), so small grids run side by side on the SMs
+// and the host launches once per step.
+struct vdi_batch {
+    std::vector<vdi_sim*> sims;
+    cudaStream_t s0 = nullptr;
+    cudaEvent_t ev0 = nullptr;
+    std::vector<cudaEvent_t> evd;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<double> gdts;
+};
+
+namespace {
+
+void batch_drop_graph(vdi_batch* B) {
+    if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    B->gexec = nullptr;
+    B->graph = nullptr;
+}
+
+int batch_capture(vdi_batch* B, const double* dts) {
+    batch_drop_graph(B);
+    for (size_t k = 0; k < B->sims.size(); k++) VDI_TRY(update_visc(B->sims[k], dts[k]));
+    VDI_CUDA(cudaStreamBeginCapture(B->s0, cudaStreamCaptureModeRelaxed));
+    int st = VDI_OK;
+    cudaError_t e = cudaEventRecord(B->ev0, B->s0);
+    for (size_t k = 0; k < B->sims.size() && st == VDI_OK && e == cudaSuccess; k++) {
+        vdi_sim* S = B->sims[k];
+        e = cudaStreamWaitEvent(S->s, B->ev0, 0);
+        if (e == cudaSuccess) st = enqueue_step(S, dts[k]);
+        if (st == VDI_OK && e == cudaSuccess) e = cudaEventRecord(B->evd[k], S->s);
+        if (st == VDI_OK && e == cudaSuccess) e = cudaStreamWaitEvent(B->s0, B->evd[k], 0);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(B->s0, &g);
+    if (st != VDI_OK || e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (st != VDI_OK) return st;
+        VDI_CUDA(e != cudaSuccess ? e : e2);
+    }
+    B->graph = g;
+    VDI_CUDA(cudaGraphInstantiate(&B->gexec, g, 0));
+    B->gdts.assign(dts, dts + B->sims.size());
+    return VDI_OK;
+}
+
+}  // namespace
+
+int vdi_batch_create(const vdi_params* prms, int count, vdi_batch** out) {
+    if (!prms || count < 1 || !out) return VDI_ERR_INVALID_ARGUMENT;
+    vdi_batch* B = new vdi_batch();
+    auto fail = [&](int st) {
+        vdi_batch_destroy(B);
+        return st;
+    };
+    if (cudaStreamCreateWithFlags(&B->s0, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&B->ev0, cudaEventDisableTiming) != cudaSuccess)
+        return fail(VDI_ERR_CUDA);
+    for (int k = 0; k < count; k++) {
+        vdi_sim* S = nullptr;
+        int st = vdi_sim_create(prms + k, nullptr, &S);
+        if (st != VDI_OK) return fail(st);
+        B->sims.push_back(S);
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail(VDI_ERR_CUDA);
+        B->evd.push_back(ev);
+    }
+    *out = B;
+    return VDI_OK;
+}
+
+int vdi_batch_destroy(vdi_batch* B) {
+    if (!B) return VDI_OK;
+    if (B->s0) cudaStreamSynchronize(B->s0);
+    batch_drop_graph(B);
+    for (auto S : B->sims) vdi_sim_destroy(S);
+    for (auto e : B->evd) cudaEventDestroy(e);
+    if (B->ev0) cudaEventDestroy(B->ev0);
+    if (B->s0) cudaStreamDestroy(B->s0);
+    delete B;
+    return VDI_OK;
+}
+
+int vdi_batch_size(const vdi_batch* B) { return B ? int(B->sims.size()) : 0; }
+
+int vdi_batch_sim(vdi_batch* B, int k, vdi_sim** out) {
+    if (!B || !out || k < 0 || k >= int(B->sims.size())) return VDI_ERR_INVALID_ARGUMENT;
+    *out = B->sims[k];
+    return VDI_OK;
+}
+
+int vdi_batch_init_fields(vdi_batch* B) {
+    if (!B) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaStreamSynchronize(B->s0));
+    for (auto S : B->sims) VDI_TRY(vdi_sim_init_fields(S));
+    return VDI_OK;
+}
+
+int vdi_batch_autotune(vdi_batch* B, vdi_tune* out) {
+    if (!B) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaStreamSynchronize(B->s0));
+    batch_drop_graph(B);
+    for (size_t k = 0; k < B->sims.size(); k++) VDI_TRY(vdi_sim_autotune(B->sims[k], out ? out + k : nullptr));
+    return VDI_OK;
+}
+
+int vdi_batch_step_forward(vdi_batch* B, const double* dts, int nsteps) {
+    if (!B || !dts || nsteps < 0) return VDI_ERR_INVALID_ARGUMENT;
+    for (size_t k = 0; k < B->sims.size(); k++)
+        if (!(dts[k] > 0)) return VDI_ERR_INVALID_ARGUMENT;
+    bool same = B->gexec && std::equal(B->gdts.begin(), B->gdts.end(), dts);
+    for (auto S : B->sims) destroy_graph(S);
+    if (!same) VDI_TRY(batch_capture(B, dts));
+    for (int q = 0; q < nsteps; q++) VDI_CUDA(cudaGraphLaunch(B->gexec, B->s0));
+    VDI_CUDA(cudaStreamSynchronize(B->s0));
+    for (size_t k = 0; k < B->sims.size(); k++) {
+        B->sims[k]->steps += nsteps;
+        int st = check_errors(B->sims[k]);
+        if (st != VDI_OK) {
+            std::string d = vdi_last_error();
+            set_error("batch simulation %zu: %s", k, d.c_str());
+            return st;
+        }
+    }
+    return VDI_OK;
+}

@@ -519,28 +519,33 @@ __global__ void k_guess2_finish(GuessHist* h, const double* d_time, int* err) {
 }
 
 // --------------------------------------------------------------- launch
-static dim3 cell_grid(int m, int n) { return dim3((m + 31) / 32, (n + 7) / 8); }
-static const dim3 CELL_BLOCK(32, 8);
+static dim3 cell_block(const Grid& g) {
+    return g.blk_x > 0 ? dim3(g.blk_x, g.blk_y) : dim3(32, 8);
+}
+static dim3 cell_grid(const Grid& g, int extra = 0) {
+    dim3 b = cell_block(g);
+    return dim3((g.m + extra + b.x - 1) / b.x, (g.n + extra + b.y - 1) / b.y);
+}
 
 int launch_stage1(cudaStream_t s, const Grid& g, const Fields& f, double dt) {
-    k_stage1<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, dt);
+    k_stage1<<<cell_grid(g), cell_block(g), 0, s>>>(g, f, dt);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_stage2(cudaStream_t s, const Grid& g, const Fields& f) {
-    k_stage2<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f);
+    k_stage2<<<cell_grid(g), cell_block(g), 0, s>>>(g, f);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_stage34(cudaStream_t s, const Grid& g, const Fields& f, double dt) {
-    k_stage34<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, dt);
+    k_stage34<<<cell_grid(g), cell_block(g), 0, s>>>(g, f, dt);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_stage5_src(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double dt, double* src) {
-    k_stage5_src<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, gs, dt, src);
+    k_stage5_src<<<cell_grid(g), cell_block(g), 0, s>>>(g, f, gs, dt, src);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_mac_advect(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, const double* q, double dt,
                       double* d_time) {
-    k_mac_advect<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, gs, q, dt, d_time);
+    k_mac_advect<<<cell_grid(g), cell_block(g), 0, s>>>(g, f, gs, q, dt, d_time);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_inviscid_bc(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double dt) {
@@ -554,17 +559,17 @@ int launch_viscous_bc(cudaStream_t s, const Grid& g, const Fields& f, const Gas&
 }
 int launch_visc_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double vfx, double vfy,
                     double* su, double* sv) {
-    k_visc_rhs<<<cell_grid(g.m, g.n), CELL_BLOCK, 0, s>>>(g, f, gs, vfx, vfy, su, sv);
+    k_visc_rhs<<<cell_grid(g), cell_block(g), 0, s>>>(g, f, gs, vfx, vfy, su, sv);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_fem_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, CellView c0, CellView c1, double dt,
                    double a_cc_edge, double a_cc_mid, double* src) {
-    k_fem_rhs<<<cell_grid(g.m + 1, g.n + 1), CELL_BLOCK, 0, s>>>(g, f, gs, c0, c1, dt, a_cc_edge, a_cc_mid, src);
+    k_fem_rhs<<<cell_grid(g, 1), cell_block(g), 0, s>>>(g, f, gs, c0, c1, dt, a_cc_edge, a_cc_mid, src);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c0, CellView c1, const double* z,
                       double dt) {
-    k_vel_update<<<cell_grid(g.m + 1, g.n + 1), CELL_BLOCK, 0, s>>>(g, f, c0, c1, z, dt);
+    k_vel_update<<<cell_grid(g, 1), cell_block(g), 0, s>>>(g, f, c0, c1, z, dt);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_guess2(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,

@@ -10,6 +10,7 @@ namespace vdi {
 struct Grid {
     int m, n;
     int x_sym, implicit_visc;
+    int blk_x, blk_y;          // launch shape of the per-cell kernels (autotuned)
     double ax, ay, bx, by, dx, dy, xsp, ysp, xxsp, yysp;
     double rho, rhoinv, mu, muinv, viscfac;
 };

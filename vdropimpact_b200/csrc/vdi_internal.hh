@@ -93,6 +93,12 @@ int mg_create(int kind, int m, int n, double c1, double c2, int x_sym, MG** out)
 void mg_destroy(MG* mg);
 /** Re-derives the viscous coefficients (visco_impl::setup_and_solve
  * re-setup when vfx changes, visco_impl.cc:26-30). */
+/** Bytes below which levels run in the single-CTA cycle (rebuilds). */
+int mg_set_cta_limit(MG* mg, size_t bytes);
+size_t mg_cta_limit(const MG* mg);
+/** Tiled (per-launch) levels of the hierarchy for a precision; -1 for the
+ * general hierarchy. */
+int mg_tiled_levels(const MG* mg, int precision);
 int mg_set_visc(MG* mg, double vfx, double vfy);
 /** Solves A z = b on the stream. z holds the initial guess. Returns a
  * VDI_* status; eager mode reads the convergence state on the host. */
