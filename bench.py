@@ -4,11 +4,15 @@ fluid solve on the 2048x1024 liquid-deposition workload (100 cSt drop,
 
 One step = fluid_2d::step_forward: gas-layer Newton/tridiagonal update,
 Godunov advection, MAC multigrid projection, two implicit viscous multigrid
-solves, FEM multigrid projection. Two solver configurations run back to
-back on the same workload:
-  plain  - FP64 V-cycles, time-extrapolated initial guess (the reference's
-           method on the GPU)
-  fast   - FP32 V-cycles inside FP64 iterative refinement (the headline)
+solves, FEM multigrid projection. Solver configurations timed on the same
+workload:
+  plain     - FP64 V-cycles, linear time-extrapolated initial guess (the
+              reference's method on the GPU)
+  fast      - the headline: by default FP64 V-cycles with the quadratic
+              time-extrapolated guess, the fastest measured configuration
+  variants  - FP32 coarse-grid corrections (hybrid), FP32 V-cycles in FP64
+              iterative refinement (mixed), and the learned U-Net guess with
+              the refined V-cycles (learned_mixed), over fewer steps
 `value` is the headline configuration's steps/s, summed over ranks (each
 rank runs an independent replica of the simulation).
 
@@ -37,7 +41,7 @@ WORKLOAD = "ld_vis100 drop impact, 2048x1024 liquid grid, 2048-cell gas layer"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", default="2048x1024")
@@ -46,8 +50,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only", default="", help="run only 'plain' or 'fast' (profiling)")
     ap.add_argument("--eager", action="store_true", help="launch kernels without CUDA graphs (profiling)")
-    ap.add_argument("--fast-precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--fast-precision", default="fp64", choices=["fp64", "mixed", "hybrid"])
     ap.add_argument("--fast-guess", default="quadratic", choices=["linear", "quadratic", "learned"])
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the other solver configurations (hybrid, mixed, learned+mixed)")
     return ap.parse_args()
 
 
@@ -191,10 +197,13 @@ def run_reference_arm(args, ws, rank):
 
 
 # ----------------------------------------------------------------- ours
-def time_config(V, torch, text, args, precision, guess, stream, ws, clocks=None):
+def time_config(V, torch, text, args, precision, guess, stream, ws, clocks=None, net=None, steps=None):
     f = V.Fluid2D(text, mg_rtol=args.rtol, mg_precision=precision, mg_guess=guess, graph=not args.eager,
                   stream=stream)
+    if net is not None:
+        f.attach_unet(net[0], net[1])
     f.init_fields()
+    nsteps = steps or args.steps
     dt = f.frame_dt()
     f.step_forward(dt, args.warmup)
     f.stats(reset=True)
@@ -205,7 +214,7 @@ def time_config(V, torch, text, args, precision, guess, stream, ws, clocks=None)
     if clocks:
         clocks.start()
     e0.record(stream)
-    f.step_forward(dt, args.steps)
+    f.step_forward(dt, nsteps)
     e1.record(stream)
     e1.synchronize()
     ck = clocks.stop() if clocks else None
@@ -216,6 +225,21 @@ def time_config(V, torch, text, args, precision, guess, stream, ws, clocks=None)
     solves = sum(st["solves"].values())
     vc = {k: st["vcycles"][k] / max(st["solves"][k], 1) for k in st["vcycles"]}
     return f, dt, ms, vc, st, ck, solves
+
+
+def train_guess_net(V, torch, text, args, factor=4):
+    """A U-Net for the learned MAC guess, trained on the GPU on (residual,
+    error) pairs harvested from the first steps of the same workload."""
+    from vdropimpact_b200 import learned
+    base = V.Fluid2D(text, mg_rtol=args.rtol, mg_guess="quadratic")
+    base.init_fields()
+    dt = base.frame_dt()
+    mac = V.MgsMac(base.m, base.n, base.dx, base.dy)
+    xs, ts = learned.harvest(base, 48, dt, factor, mac)
+    net = learned.UNet(base.n // factor, base.m // factor, batch=8, seed=11)
+    learned.train(net, xs, ts, iters=400, lr=3e-4, batch=8)
+    base.close()
+    return net, factor
 
 
 def measured_peak_gbs():
@@ -250,12 +274,19 @@ def roofline(V, torch, args):
             "traffic": CC_POST_DRAM_BYTES, "algorithmic_bytes": nbytes, "ms_per_launch": ms}
 
 
-def e2e_run(V, torch, f, dt, stream, steps, ws):
-    """The same metric through the public API: each step is one
+def e2e_run(V, torch, text, args, stream, steps, ws):
+    """The same metric through the public API over the same step window as
+    the timed region (a fresh simulation of the headline configuration, W
+    warm-up steps from init, then the timed steps): each step is one
     Fluid2D.step_forward call (C-ABI vdi_sim_step_forward with the host
     timestep, which returns the step's device-side status), followed by a
     device-to-host read of the step's result, the gas-layer height h(x) and
     gas pressure, into pinned memory."""
+    f = V.Fluid2D(text, mg_rtol=args.rtol, mg_precision=args.fast_precision, mg_guess=args.fast_guess,
+                  graph=not args.eager, stream=stream)
+    f.init_fields()
+    dt = f.frame_dt()
+    f.step_forward(dt, args.warmup)
     dh, nh = f.device_field(3)
     dp, npg = f.device_field(4)
     hbuf = torch.empty(nh, dtype=torch.float64, pin_memory=True)
@@ -275,6 +306,7 @@ def e2e_run(V, torch, f, dt, stream, steps, ws):
     e1.record(stream)
     e1.synchronize()
     ms = dist_max(e0.elapsed_time(e1), ws)
+    f.close()
     return ms, 8, 8 * (nh + npg)
 
 
@@ -322,9 +354,10 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if args.fast_precision == "fp64" else "f64+f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": args.grid, "mg_rtol": args.rtol,
-                   "solver": "FP32 V-cycles in FP64 refinement, time-extrapolated guess, CUDA-graph step",
+                   "solver": f"{args.fast_precision} V-cycles, {args.fast_guess} time-extrapolated guess, "
+                             "CUDA-graph step",
                    "l2": "per-step working set (~0.9 GB) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{ws}"},
         "clocks": head["clocks"],
@@ -336,11 +369,26 @@ def main():
         line["plain_fp64"] = {"steps_per_s": ws * 1e3 * args.steps / p["ms"], "ms_per_step": p["ms"] / args.steps,
                               "vcycles_per_solve": p["vc"]}
         line["speedup_vs_plain_fp64"] = p["ms"] / head["ms"]
+    if not args.no_variants and not args.only and ws == 1:
+        # the other solver configurations of the metric, on the same workload:
+        # FP32 coarse-grid corrections, FP32 V-cycles in FP64 refinement, and
+        # the learned guess with the refined V-cycles
+        vsteps = args.steps
+        variants = {}
+        for name, prec, guess in (("hybrid_quadratic", "hybrid", "quadratic"),
+                                  ("mixed_quadratic", "mixed", "quadratic"),
+                                  ("learned_mixed", "mixed", "learned")):
+            net = train_guess_net(V, torch, text, args) if guess == "learned" else None
+            fv, _, msv, vcv, _, _, _ = time_config(V, torch, text, args, prec, guess, stream, ws, net=net,
+                                                  steps=vsteps)
+            variants[name] = {"steps_per_s": 1e3 * vsteps / msv, "steps": vsteps, "vcycles_per_solve": vcv}
+            fv.close()
+        line["variants"] = variants
     f, dt = keep
     line["roofline"] = roofline(V, torch, args)
     if not args.no_e2e:
-        e2e_steps = max(3, min(args.steps, 50))
-        ms, bi, bo = e2e_run(V, torch, f, dt, stream, e2e_steps, ws)
+        e2e_steps = args.steps
+        ms, bi, bo = e2e_run(V, torch, text, args, stream, e2e_steps, ws)
         line["e2e"] = {"value": ws * 1e3 * e2e_steps / ms, "unit": "steps/s", "h2d_bytes_per_step": bi,
                        "d2h_bytes_per_step": bo}
     f.close()

@@ -74,7 +74,9 @@ typedef struct vdi_params {
 
 enum vdi_mg_precision {
     VDI_MG_FP64 = 0,          /* FP64 V-cycles */
-    VDI_MG_MIXED = 1          /* FP32 V-cycles inside FP64 iterative refinement */
+    VDI_MG_MIXED = 1,         /* FP32 V-cycles inside FP64 iterative refinement */
+    VDI_MG_HYBRID = 2         /* FP64 finest level (smoothing, residual, stop test)
+                                 with FP32 coarse-grid corrections */
 };
 enum vdi_mg_guess {
     VDI_GUESS_EXTRAPOLATE = 0, /* linear time extrapolation (mgs_common.cc:17-50) */

@@ -76,7 +76,7 @@ def test_visc_apply_equals_accessors(V, x_sym, horiz):
     assert _rel(y, A @ z) < 1e-14
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "hybrid"])
 @pytest.mark.parametrize("m,n", [(256, 128), (512, 256)])
 def test_mac_solve_gaussians(V, m, n, prec):
     torch = _torch()
@@ -95,7 +95,7 @@ def test_mac_solve_gaussians(V, m, n, prec):
     assert _rel(z, zd) < 1e-6
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "hybrid"])
 def test_fem_solve(V, prec):
     torch = _torch()
     M, N = 257, 129
@@ -119,7 +119,7 @@ def test_fem_solve(V, prec):
 
 
 @pytest.mark.parametrize("x_sym,horiz", [(True, True), (True, False), (False, False)])
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "hybrid"])
 def test_visc_solve(V, x_sym, horiz, prec):
     torch = _torch()
     m, n, vfx, vfy = 256, 128, 0.4, 0.4

@@ -122,3 +122,23 @@ def test_free_running_steps_odd_grid(V):
     f.step_forward(dt, 10)
     e = rel_errors(f.state(), o.state())
     assert max(e.values()) < TOL, e
+
+
+@pytest.mark.parametrize("prec,guess", [("hybrid", "quadratic"), ("mixed", "linear")])
+def test_free_running_precision_modes(V, prec, guess):
+    """40 steps with FP32 coarse-grid corrections (hybrid) or FP32 V-cycles in
+    FP64 refinement (mixed): every solve still stops on the FP64 residual, so
+    the fields agree with the oracle within the same bound."""
+    txt = cfg_text()
+    o = vo.Oracle(vo.parse_cfg(txt))
+    o.init_fields()
+    dt = o.prm.frame_dt()
+    f = V.Fluid2D(txt, mg_rtol=1e-10, mg_precision=prec, mg_guess=guess, graph=True)
+    f.init_fields()
+    for k in range(40):
+        o.step(dt)
+    f.step_forward(dt, 40)
+    e = rel_errors(f.state(), o.state())
+    assert max(e.values()) < TOL, e
+    st = f.stats()
+    assert max(st["last_rel_res"].values()) <= 1e-10

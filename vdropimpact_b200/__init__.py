@@ -26,7 +26,8 @@ from ._abi import (VDI_MG_FP64, VDI_MG_MIXED, VDI_GUESS_EXTRAPOLATE, VDI_GUESS_L
 __all__ = ["Fluid2D", "MgsMac", "MgsFem", "ViscoImpl", "TriSolve", "VdiError", "params_from_cfg",
            "VDI_MG_FP64", "VDI_MG_MIXED", "VDI_GUESS_EXTRAPOLATE", "VDI_GUESS_LEARNED"]
 
-_PREC = {"fp64": VDI_MG_FP64, "mixed": VDI_MG_MIXED, VDI_MG_FP64: VDI_MG_FP64, VDI_MG_MIXED: VDI_MG_MIXED}
+_PREC = {"fp64": VDI_MG_FP64, "mixed": VDI_MG_MIXED, "hybrid": _abi.VDI_MG_HYBRID, VDI_MG_FP64: VDI_MG_FP64,
+         VDI_MG_MIXED: VDI_MG_MIXED, _abi.VDI_MG_HYBRID: _abi.VDI_MG_HYBRID}
 
 
 def _torch():

@@ -26,6 +26,7 @@ VDI_ERR_NOT_READY = 10
 
 VDI_MG_FP64 = 0
 VDI_MG_MIXED = 1
+VDI_MG_HYBRID = 2
 VDI_GUESS_EXTRAPOLATE = 0
 VDI_GUESS_LEARNED = 1
 VDI_GUESS_QUADRATIC = 2

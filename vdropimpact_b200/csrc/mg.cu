@@ -197,42 +197,38 @@ __device__ __forceinline__ T op_relaxed(const OP& c, const T* w, T bv, int P, in
 
 /** Bilinear cell-centred prolongation of the coarse correction to fine cell
  * (i,j); ghost values are g * (boundary value) on each side. */
-template <typename T>
-__device__ __forceinline__ T cc_interp(const CCc<T>& f, const T* zc, int i, int j) {
+template <typename T, typename TC>
+__device__ __forceinline__ T cc_interp(const CCc<T>& f, const TC* zc, int i, int j) {
     const int mc = f.m >> 1, nc = f.n >> 1;
     int I = i >> 1, J = j >> 1;
     int sx = (i & 1) ? 1 : -1, sy = (j & 1) ? 1 : -1;
     int Ix = I + sx, Jy = J + sy;
     bool xo = Ix < 0 || Ix >= mc, yo = Jy < 0 || Jy >= nc;
     T gx = T(sx < 0 ? f.gL : f.gR), gy = T(sy < 0 ? f.gD : f.gU);
-    T c00 = zc[I + mc * J];
-    T c10 = xo ? gx * c00 : zc[Ix + mc * J];
-    T c01 = yo ? gy * c00 : zc[I + mc * Jy];
+    T c00 = T(zc[I + mc * J]);
+    T c10 = xo ? gx * c00 : T(zc[Ix + mc * J]);
+    T c01 = yo ? gy * c00 : T(zc[I + mc * Jy]);
     T c11;
     if (xo && yo) c11 = gx * gy * c00;
     else if (xo) c11 = gx * c01;
     else if (yo) c11 = gy * c10;
-    else c11 = zc[Ix + mc * Jy];
+    else c11 = T(zc[Ix + mc * Jy]);
     return T(0.5625) * c00 + T(0.1875) * (c10 + c01) + T(0.0625) * c11;
 }
 
 /** Bilinear prolongation of node-centred corrections to fine node (i,j). */
-template <typename T>
-__device__ __forceinline__ T fem_interp(const FEMc<T>& f, const T* zc, int i, int j) {
+template <typename T, typename TC>
+__device__ __forceinline__ T fem_interp(const FEMc<T>& f, const TC* zc, int i, int j) {
     if (j == 0) return T(0);
     const int Mc = (f.M - 1) / 2 + 1;
     int I = i >> 1, J = j >> 1;
     bool ox = i & 1, oy = j & 1;
-    T c00 = zc[I + Mc * J];
+    T c00 = T(zc[I + Mc * J]);
     if (!ox && !oy) return c00;
-    if (ox && !oy) return T(0.5) * (c00 + zc[I + 1 + Mc * J]);
-    if (!ox && oy) return T(0.5) * (c00 + zc[I + Mc * (J + 1)]);
-    return T(0.25) * (c00 + zc[I + 1 + Mc * J] + zc[I + Mc * (J + 1)] + zc[I + 1 + Mc * (J + 1)]);
+    if (ox && !oy) return T(0.5) * (c00 + T(zc[I + 1 + Mc * J]));
+    if (!ox && oy) return T(0.5) * (c00 + T(zc[I + Mc * (J + 1)]));
+    return T(0.25) * (c00 + T(zc[I + 1 + Mc * J]) + T(zc[I + Mc * (J + 1)]) + T(zc[I + 1 + Mc * (J + 1)]));
 }
-template <typename T>
-__device__ __forceinline__ T op_interp(const CCc<T>& c, const T* zc, int i, int j) { return cc_interp(c, zc, i, j); }
-template <typename T>
-__device__ __forceinline__ T op_interp(const FEMc<T>& c, const T* zc, int i, int j) { return fem_interp(c, zc, i, j); }
 
 /** P^T r at coarse node (I,J) from a residual array with origin (ox,oy) and
  * pitch P; zero on the Dirichlet bottom row. */
@@ -255,14 +251,14 @@ __device__ __forceinline__ T fem_restrict_at(int M, int N, const T* r, int P, in
 }
 
 // ------------------------------------------------------- fused tile kernels
-template <typename T>
+template <typename T, typename TC = T>
 struct TileArgs {
     const T* zin;      // iterate read (PRE: unless zero_init; POST: before the correction)
     T* zout;           // iterate written; never the array zin points to, because
                        // neighbouring tiles read zin as their halo concurrently
     const T* b;
-    T* bc;             // PRE: coarse source out
-    const T* zc;       // POST: coarse correction in
+    TC* bc;            // PRE: coarse source out (the coarse levels' precision)
+    const TC* zc;      // POST: coarse correction in
     int zero_init;     // PRE: z starts from zero (coarse levels)
     int norm;          // POST: residual norm + decision
     Reduce rd;
@@ -271,189 +267,6 @@ struct TileArgs {
     cudaGraphConditionalHandle h;
 };
 
-template <int KIND, int MODE, int NS>
-struct TileShape {
-    static constexpr int NCOL = KIND == 0 ? 2 : 4;
-    static constexpr int K = NS * NCOL;               // colour phases
-    static constexpr int ZH = (MODE == 0 && KIND == 1) ? K + 2 : K + 1;  // z halo
-    static constexpr int BH = ZH - 1;                 // b halo
-};
-
-/** Tile shape: TX x TY interior points per CTA of NT threads. The large
- * shape serves the finest levels; the small one keeps coarser multi-CTA
- * levels spread over all SMs. */
-template <typename T, int KIND, int SMALL>
-struct TileDims;
-template <> struct TileDims<double, 0, 0> { static constexpr int TX = 64, TY = 16, NT = 512; };
-template <> struct TileDims<float, 0, 0> { static constexpr int TX = 64, TY = 32, NT = 512; };
-template <> struct TileDims<double, 1, 0> { static constexpr int TX = 64, TY = 32, NT = 512; };
-template <> struct TileDims<float, 1, 0> { static constexpr int TX = 64, TY = 32, NT = 512; };
-template <typename T, int KIND> struct TileDims<T, KIND, 1> { static constexpr int TX = 32, TY = 16, NT = 256; };
-
-template <typename T, int KIND, int MODE, int NS, int SMALL>
-constexpr size_t tile_smem() {
-    using S = TileShape<KIND, MODE, NS>;
-    using D = TileDims<T, KIND, SMALL>;
-    size_t zb = size_t(D::TX + 2 * S::ZH) * (D::TY + 2 * S::ZH);
-    size_t bb = size_t(D::TX + 2 * S::BH) * (D::TY + 2 * S::BH);
-    size_t rb = (MODE == 0 && KIND == 1) ? size_t(D::TX + 2) * (D::TY + 2) : 0;
-    return (zb + bb + rb) * sizeof(T);
-}
-
-/** One sweep colour over the points of region [xs,xs+W) x [ys,ys+H) that lie
- * in the grid. Inlined into a fully unrolled phase loop, so W and H are
- * compile-time constants there. */
-template <typename T, int KIND, int NT, class OP>
-__device__ __forceinline__ void tile_phase(const OP& c, T* zt, const T* bt, int ZW, int zx, int zy, int BW, int bx,
-                                           int by, int color, int xs, int ys, int W, int H) {
-    const int M = op_m(c), N = op_n(c);
-    if (KIND == 0) {
-        const int half = (W + 1) >> 1, tot = H * half;
-#pragma unroll 4
-        for (int t = threadIdx.x; t < tot; t += NT) {
-            int row = t / half, c2 = t - row * half;
-            int j = ys + row;
-            int i = xs + 2 * c2 + ((color ^ (xs + j)) & 1);
-            if (i >= xs + W || i < 0 || i >= M || j < 0 || j >= N) continue;
-            T* w = zt + (i - zx) + ZW * (j - zy);
-            *w = op_relaxed(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
-        }
-    } else {
-        const int ci = color & 1, cj = color >> 1;
-        const int W2 = (W + 1) >> 1, H2 = (H + 1) >> 1, tot = W2 * H2;
-        const int pi = (ci ^ xs) & 1, pj = (cj ^ ys) & 1;
-#pragma unroll 4
-        for (int t = threadIdx.x; t < tot; t += NT) {
-            int jr = t / W2, ir = t - jr * W2;
-            int j = ys + 2 * jr + pj, i = xs + 2 * ir + pi;
-            if (i >= xs + W || j >= ys + H || i < 0 || i >= M || j < 0 || j >= N) continue;
-            T* w = zt + (i - zx) + ZW * (j - zy);
-            *w = op_relaxed(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
-        }
-    }
-}
-
-/** Loads a (W x H) window with origin (ox,oy) of a grid array into shared
- * memory (zero outside the grid; with zc, adds the prolonged coarse
- * correction). All loads of a thread are issued before any store so they
- * are in flight together. */
-template <typename T, int W, int H, int NT, int MODE, class OP>
-__device__ __forceinline__ void tile_load(const OP& c, T* dst, const T* src, const T* zc, int ox, int oy,
-                                          bool zero) {
-    constexpr int NL = (W * H + NT - 1) / NT;
-    const int M = op_m(c), N = op_n(c);
-    T v[NL];
-#pragma unroll
-    for (int q = 0; q < NL; q++) {
-        int t = threadIdx.x + q * NT;
-        int jj = t / W, ii = t - jj * W;
-        int i = ox + ii, j = oy + jj;
-        bool in = t < W * H && i >= 0 && i < M && j >= 0 && j < N;
-        v[q] = (in && !zero) ? src[i + M * j] : T(0);
-        if (MODE == 1 && in) v[q] += op_interp(c, zc, i, j);
-    }
-#pragma unroll
-    for (int q = 0; q < NL; q++) {
-        int t = threadIdx.x + q * NT;
-        if (t < W * H) dst[t] = v[q];
-    }
-}
-
-template <typename T, int KIND, int MODE, int NS, int SMALL, class OP>
-__global__ void __launch_bounds__(TileDims<T, KIND, SMALL>::NT) mg_tile(OP c, TileArgs<T> a) {
-    using S = TileShape<KIND, MODE, NS>;
-    using D = TileDims<T, KIND, SMALL>;
-    constexpr int TX = D::TX, TY = D::TY, NT = D::NT, ZH = S::ZH, BH = S::BH, K = S::K, NCOL = S::NCOL;
-    constexpr int ZW = TX + 2 * ZH, ZHT = TY + 2 * ZH, BW = TX + 2 * BH, BHT = TY + 2 * BH;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    T* zt = reinterpret_cast<T*>(sm_raw);
-    T* bt = zt + ZW * ZHT;
-    T* rt = bt + BW * BHT;
-    const int M = op_m(c), N = op_n(c);
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int zx = x0 - ZH, zy = y0 - ZH, bx = x0 - BH, by = y0 - BH;
-    tile_load<T, ZW, ZHT, NT, MODE>(c, zt, a.zin, a.zc, zx, zy, MODE == 0 && a.zero_init);
-    tile_load<T, BW, BHT, NT, 0>(c, bt, a.b, nullptr, bx, by, false);
-    __syncthreads();
-#pragma unroll
-    for (int k = 1; k <= K; k++) {
-        const int ph = (k - 1) % NCOL;
-        const int color = MODE == 0 ? ph : NCOL - 1 - ph;
-        const int r = ZH - k;
-        tile_phase<T, KIND, NT>(c, zt, bt, ZW, zx, zy, BW, bx, by, color, x0 - r, y0 - r, TX + 2 * r, TY + 2 * r);
-        __syncthreads();
-    }
-    // interior back to global memory
-#pragma unroll 4
-    for (int t = threadIdx.x; t < TX * TY; t += NT) {
-        int jj = t / TX, ii = t - jj * TX;
-        int i = x0 + ii, j = y0 + jj;
-        if (i < M && j < N) a.zout[i + M * j] = zt[(i - zx) + ZW * (j - zy)];
-    }
-    if (MODE == 0) {
-        if (KIND == 0) {
-            const int mc = M >> 1, nc = N >> 1;
-            for (int t = threadIdx.x; t < (TX / 2) * (TY / 2); t += NT) {
-                int q = t / (TX / 2);
-                int I = x0 / 2 + (t - q * (TX / 2)), J = y0 / 2 + q;
-                if (I >= mc || J >= nc) continue;
-                T s = 0;
-#pragma unroll
-                for (int dj = 0; dj < 2; dj++)
-#pragma unroll
-                    for (int di = 0; di < 2; di++) {
-                        int i = 2 * I + di, j = 2 * J + dj;
-                        const T* w = zt + (i - zx) + ZW * (j - zy);
-                        s += op_resid(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
-                    }
-                a.bc[I + mc * J] = T(0.25) * s;
-            }
-        } else {
-            constexpr int RW = TX + 2, RH = TY + 2;
-            for (int t = threadIdx.x; t < RW * RH; t += NT) {
-                int jj = t / RW, ii = t - jj * RW;
-                int i = x0 - 1 + ii, j = y0 - 1 + jj;
-                T v = 0;
-                if (i >= 0 && i < M && j >= 0 && j < N) {
-                    const T* w = zt + (i - zx) + ZW * (j - zy);
-                    v = op_resid(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j);
-                }
-                rt[t] = v;
-            }
-            __syncthreads();
-            const int Mc = (M - 1) / 2 + 1, Nc = (N - 1) / 2 + 1;
-            for (int t = threadIdx.x; t < (TX / 2) * (TY / 2); t += NT) {
-                int q = t / (TX / 2);
-                int I = x0 / 2 + (t - q * (TX / 2)), J = y0 / 2 + q;
-                if (I >= Mc || J >= Nc) continue;
-                a.bc[I + Mc * J] = fem_restrict_at(M, N, rt, RW, x0 - 1, y0 - 1, I, J);
-            }
-        }
-    } else if (a.norm) {
-        double s = 0;
-        for (int t = threadIdx.x; t < TX * TY; t += NT) {
-            int jj = t / TX, ii = t - jj * TX;
-            int i = x0 + ii, j = y0 + jj;
-            if (i < M && j < N) {
-                const T* w = zt + (i - zx) + ZW * (j - zy);
-                double r = double(op_resid(c, w, bt[(i - bx) + BW * (j - by)], ZW, i, j));
-                s += r * r;
-            }
-        }
-        s = block_sum(s);
-        double total;
-        if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
-    }
-}
-
-// ------------------------------------------ red-black split cell-centred tile
-// The 5-point systems use their own tile kernel: a 64 x 64 window stored as
-// two colour arrays, S_c[jj][k] = window point (2k + p, jj) of colour c, so a
-// warp updates one colour-row with 32 consecutive shared-memory words and its
-// four neighbours are also consecutive words. Every colour phase updates the
-// whole window; points within K rings of the window edge go stale one ring per
-// phase, which the halo of ZH = K + 1 rings keeps out of the interior results.
-// Tiles away from the grid edge skip all boundary tests.
 template <typename T, int NS>
 struct CCTile {
     static constexpr int CW = 64, CH = 64, KW = CW / 2;
@@ -466,8 +279,8 @@ struct CCTile {
 /** MODE 0: NS sweeps from zin (or zero), residual, restriction to bc (skipped
  * when bc is null). MODE 1: zin + prolonged zc, NS sweeps, and optionally the
  * residual norm with the solve decision. Both write zout. */
-template <typename T, int MODE, int NS>
-__global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<T> a) {
+template <typename T, int MODE, int NS, typename TC = T>
+__global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<T, TC> a) {
     using G = CCTile<T, NS>;
     constexpr int CW = G::CW, CH = G::CH, KW = G::KW, ZH = G::ZH, TX = G::TX, TY = G::TY, K = G::K;
     constexpr int NW = G::NW, RPW = CH / NW;
@@ -569,7 +382,7 @@ __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<
                 if (I >= mc || J >= nc) continue;
                 const int ii = 2 * I - zx, jj = 2 * J - zy;
                 T s = resid(ii, jj) + resid(ii + 1, jj) + resid(ii, jj + 1) + resid(ii + 1, jj + 1);
-                a.bc[I + mc * J] = T(0.25) * s;
+                a.bc[I + mc * J] = TC(T(0.25) * s);
             }
         }
     } else if (a.norm) {
@@ -625,8 +438,8 @@ __device__ __forceinline__ T fem_off_vals(const FEMc<T>& c, int i, int j, T dl, 
     return c.fc * (dl + dr + ul + ur) + c.fey * (d + u) + c.fex * (l + r);
 }
 
-template <typename T, int MODE>
-__global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T> a) {
+template <typename T, int MODE, typename TC = T>
+__global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T, TC> a) {
     using G = FEMTile<T>;
     constexpr int QW = G::QW, QN = G::QN, ZH = G::ZH, TX = G::TX, TY = G::TY, K = G::K, NW = G::NW;
     constexpr int CH = G::CH, RW = G::RW, RH = G::RH;
@@ -732,7 +545,7 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
             const int q = t / CX;
             const int I = x0 / 2 + (t - q * CX), J = y0 / 2 + q;
             if (I >= Mc || J >= Nc) continue;
-            a.bc[I + Mc * J] = fem_restrict_at(M, N, R, RW, x0 - 1, y0 - 1, I, J);
+            a.bc[I + Mc * J] = TC(fem_restrict_at(M, N, R, RW, x0 - 1, y0 - 1, I, J));
         }
     } else if (a.norm) {
         double s = 0;
@@ -1055,58 +868,36 @@ struct LevelD {
     signed char gL, gR, gD, gU;
 };
 
-template <typename T, int KIND, int MODE, class OP>
-static void launch_tile(cudaStream_t s, const OP& c, const TileArgs<T>& a, int M, int N) {
-    using DL = TileDims<T, KIND, 0>;
-    using DS = TileDims<T, KIND, 1>;
-    long big = long((M + DL::TX - 1) / DL::TX) * ((N + DL::TY - 1) / DL::TY);
-    if (big >= 1024) {
-        dim3 grid((M + DL::TX - 1) / DL::TX, (N + DL::TY - 1) / DL::TY);
-        mg_tile<T, KIND, MODE, 2, 0, OP><<<grid, DL::NT, tile_smem<T, KIND, MODE, 2, 0>(), s>>>(c, a);
-    } else {
-        dim3 grid((M + DS::TX - 1) / DS::TX, (N + DS::TY - 1) / DS::TY);
-        mg_tile<T, KIND, MODE, 2, 1, OP><<<grid, DS::NT, tile_smem<T, KIND, MODE, 2, 1>(), s>>>(c, a);
-    }
-}
-
-template <typename T, int KIND, int MODE, class OP>
-static cudaError_t tile_attr() {
-    cudaError_t e = cudaFuncSetAttribute(mg_tile<T, KIND, MODE, 2, 0, OP>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(tile_smem<T, KIND, MODE, 2, 0>()));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(mg_tile<T, KIND, MODE, 2, 1, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(tile_smem<T, KIND, MODE, 2, 1>()));
-}
-
-template <typename T, int MODE>
-static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T>& a) {
+template <typename T, int MODE, typename TC = T>
+static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T, TC>& a) {
     using G = CCTile<T, 2>;
     dim3 grid((c.m + G::TX - 1) / G::TX, (c.n + G::TY - 1) / G::TY);
-    cc_tile<T, MODE, 2><<<grid, G::NT, G::smem, s>>>(c, a);
+    cc_tile<T, MODE, 2, TC><<<grid, G::NT, G::smem, s>>>(c, a);
 }
 
-template <typename T, int MODE>
-static void launch_fem_tile(cudaStream_t s, const FEMc<T>& c, const TileArgs<T>& a) {
+template <typename T, int MODE, typename TC = T>
+static void launch_fem_tile(cudaStream_t s, const FEMc<T>& c, const TileArgs<T, TC>& a) {
     using G = FEMTile<T>;
     dim3 grid((c.M + G::TX - 1) / G::TX, (c.N + G::TY - 1) / G::TY);
-    fem_tile<T, MODE><<<grid, G::NT, G::smem, s>>>(c, a);
+    fem_tile<T, MODE, TC><<<grid, G::NT, G::smem, s>>>(c, a);
 }
 
-template <typename T>
+template <typename T, typename TC = T>
 static cudaError_t fem_tile_attr() {
     using G = FEMTile<T>;
-    cudaError_t e = cudaFuncSetAttribute(fem_tile<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    cudaError_t e = cudaFuncSetAttribute(fem_tile<T, 0, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(G::smem));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(fem_tile<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    return cudaFuncSetAttribute(fem_tile<T, 1, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
 }
 
-template <typename T>
+template <typename T, typename TC = T>
 static cudaError_t cc_tile_attr() {
     using G = CCTile<T, 2>;
-    cudaError_t e = cudaFuncSetAttribute(cc_tile<T, 0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    cudaError_t e = cudaFuncSetAttribute(cc_tile<T, 0, 2, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(G::smem));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(cc_tile<T, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    return cudaFuncSetAttribute(cc_tile<T, 1, 2, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
 }
 
 #include "mg_general.cuh"
@@ -1371,18 +1162,12 @@ class MG {
                                       int(CTA_SMEM_LIMIT)));
         VDI_CUDA(cudaFuncSetAttribute(fem_cta_cycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(CTA_SMEM_LIMIT)));
-        VDI_CUDA((tile_attr<double, 0, 0, CCc<double>>()));
-        VDI_CUDA((tile_attr<double, 0, 1, CCc<double>>()));
-        VDI_CUDA((tile_attr<float, 0, 0, CCc<float>>()));
-        VDI_CUDA((tile_attr<float, 0, 1, CCc<float>>()));
-        VDI_CUDA((tile_attr<double, 1, 0, FEMc<double>>()));
-        VDI_CUDA((tile_attr<double, 1, 1, FEMc<double>>()));
-        VDI_CUDA((tile_attr<float, 1, 0, FEMc<float>>()));
-        VDI_CUDA((tile_attr<float, 1, 1, FEMc<float>>()));
         VDI_CUDA(cc_tile_attr<double>());
         VDI_CUDA(cc_tile_attr<float>());
+        VDI_CUDA((cc_tile_attr<double, float>()));
         VDI_CUDA(fem_tile_attr<double>());
         VDI_CUDA(fem_tile_attr<float>());
+        VDI_CUDA((fem_tile_attr<double, float>()));
         return VDI_OK;
     }
 
@@ -1477,6 +1262,39 @@ class MG {
         if (norm && nmulti64 == 0) VDI_TRY(enqueue_resid_norm(s, b, z, 1, use_cond, h));
         return VDI_OK;
     }
+    /** FP64 finest level (its smoothing, residual and norm) over FP32 coarse
+     * levels: the coarse-grid correction only has to be approximate, so its
+     * precision does not limit the FP64 residual the loop stops on. */
+    int vcycle_hybrid(cudaStream_t s, const double* b, double* z, int norm, int use_cond,
+                      cudaGraphConditionalHandle h) {
+        if (general || nmulti64 < 1 || nmulti32 < 1) return vcycle64(s, b, z, norm, use_cond, h);
+        TileArgs<double, float> a{};
+        a.zin = z;
+        a.zout = t64[0];
+        a.b = b;
+        a.bc = b32[1];
+        a.rd = rd;
+        a.ctl = ctl;
+        if (fem()) launch_fem_tile<double, 0, float>(s, femc<double>(0), a);
+        else launch_cc_tile<double, 0, float>(s, ccc<double>(0), a);
+        VDI_CUDA(cudaGetLastError());
+        VDI_TRY(vcycle<float>(s, 1, b32[1], z32[1], nmulti32, z32, b32, smem32, 1, 0, 0, 0));
+        TileArgs<double, float> p{};
+        p.zin = t64[0];
+        p.zout = z;
+        p.b = b;
+        p.zc = z32[1];
+        p.rd = rd;
+        p.ctl = ctl;
+        p.norm = norm;
+        p.use_cond = use_cond;
+        p.h = h;
+        if (fem()) launch_fem_tile<double, 1, float>(s, femc<double>(0), p);
+        else launch_cc_tile<double, 1, float>(s, ccc<double>(0), p);
+        VDI_CUDA(cudaGetLastError());
+        return VDI_OK;
+    }
+
     int vcycle32(cudaStream_t s) {
         return vcycle<float>(s, 0, b32[0], z32[0], nmulti32, z32, b32, smem32, 1, 0, 0, 0);
     }
@@ -1517,6 +1335,7 @@ class MG {
      * the residual norm of the new iterate and the solve decision. */
     int enqueue_body(cudaStream_t s, const double* b, double* z, int precision, int use_cond,
                      cudaGraphConditionalHandle h) {
+        if (precision == VDI_MG_HYBRID) return vcycle_hybrid(s, b, z, 1, use_cond, h);
         if (precision == VDI_MG_MIXED && !general) {
             VDI_TRY(vcycle32(s));
             add_f32_to_f64<<<nblk(size(0)), 256, 0, s>>>(z, z32[0], size(0));
@@ -1703,6 +1522,10 @@ int mg_residual(MG* mg, cudaStream_t s, const double* b, const double* z, double
 
 int mg_kernels_per_iteration(const MG* mg, int precision) {
     if (mg->general) return mg->gen.kernels_per_vcycle() + 1;
+    if (precision == VDI_MG_HYBRID) {
+        if (mg->nmulti64 < 1 || mg->nmulti32 < 1) precision = VDI_MG_FP64;
+        else return 2 * mg->nmulti32 + 1;
+    }
     int nm = precision == VDI_MG_MIXED ? mg->nmulti32 : mg->nmulti64;
     int k = 2 * nm + 1;                       // PRE/POST per tiled level + the coarsest
     if (precision == VDI_MG_MIXED) k += 2;    // FP64 update and residual
@@ -1885,10 +1708,6 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
                                                    int(CTA_SMEM_LIMIT));
     if (e == cudaSuccess) e = cudaFuncSetAttribute(fem_cta_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    int(CTA_SMEM_LIMIT));
-    if (e == cudaSuccess) e = tile_attr<double, 0, 0, CCc<double>>();
-    if (e == cudaSuccess) e = tile_attr<double, 0, 1, CCc<double>>();
-    if (e == cudaSuccess) e = tile_attr<double, 1, 0, FEMc<double>>();
-    if (e == cudaSuccess) e = tile_attr<double, 1, 1, FEMc<double>>();
     if (e == cudaSuccess) e = cc_tile_attr<double>();
     if (e == cudaSuccess) e = fem_tile_attr<double>();
     if (e != cudaSuccess) {
