@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--eager", action="store_true", help="launch kernels without CUDA graphs (profiling)")
     ap.add_argument("--fast-precision", default="fp64", choices=["fp64", "mixed", "hybrid"])
     ap.add_argument("--fast-guess", default="quadratic", choices=["linear", "quadratic", "learned"])
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes instead of the autotuned ones")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the other solver configurations (hybrid, mixed, learned+mixed)")
     return ap.parse_args()
@@ -202,6 +204,8 @@ def time_config(V, torch, text, args, precision, guess, stream, ws, clocks=None,
                   stream=stream)
     if net is not None:
         f.attach_unet(net[0], net[1])
+    if not args.no_tune:
+        f.autotune()
     f.init_fields()
     nsteps = steps or args.steps
     dt = f.frame_dt()
@@ -284,6 +288,8 @@ def e2e_run(V, torch, text, args, stream, steps, ws):
     gas pressure, into pinned memory."""
     f = V.Fluid2D(text, mg_rtol=args.rtol, mg_precision=args.fast_precision, mg_guess=args.fast_guess,
                   graph=not args.eager, stream=stream)
+    if not args.no_tune:
+        f.autotune()
     f.init_fields()
     dt = f.frame_dt()
     f.step_forward(dt, args.warmup)
@@ -357,7 +363,7 @@ def main():
         "vs_baseline": None, "dtype": "f64" if args.fast_precision == "fp64" else "f64+f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": args.grid, "mg_rtol": args.rtol,
                    "solver": f"{args.fast_precision} V-cycles, {args.fast_guess} time-extrapolated guess, "
-                             "CUDA-graph step",
+                             "CUDA-graph step" + ("" if args.no_tune else ", autotuned launch shapes"),
                    "l2": "per-step working set (~0.9 GB) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{ws}"},
         "clocks": head["clocks"],

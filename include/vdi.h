@@ -266,12 +266,12 @@ int vdi_mg_v_cycle(vdi_mg* mg, const double* d_b, double* d_z);
 int vdi_mg_residual(vdi_mg* mg, const double* d_b, const double* d_z, double* d_r, double* norm);
 /* y = A z, the operator of the problem class (a_cc*z + mul_a). */
 int vdi_mg_apply(vdi_mg* mg, const double* d_z, double* d_y);
-/* Measurement helper: launches the finest-level smoothing kernel of one
- * V-cycle (which = 0 the pre-smoothing/restriction kernel, 1 the
- * prolongation/post-smoothing kernel) iters times on d_b, d_z between two
- * CUDA events on the system's stream, and returns the mean duration per
- * launch and the kernel's algorithmic bytes per launch (each input and output
- * array read or written once). */
+/* Measurement helper: launches, iters times on d_b, d_z between two CUDA
+ * events on the system's stream, which = 0 the finest-level
+ * pre-smoothing/restriction kernel, 1 the finest prolongation/post-smoothing
+ * kernel, 2 a whole FP64 V-cycle (the ms per V-cycle that mg_test.cc:36-43
+ * reports), 3 the single-CTA coarse cycle alone; returns the mean duration
+ * and the algorithmic bytes per launch (0 for which = 3). */
 int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
                    double* bytes_per_launch);
 

@@ -37,6 +37,7 @@ static constexpr int MAXLEV = 16;
 static constexpr int CTA_THREADS = 1024;
 static constexpr size_t CTA_SMEM_LIMIT = 200 * 1024;
 static constexpr int MAX_PARTIALS = 8192;
+static constexpr int DIRECT_MAX = 256;
 
 // ------------------------------------------------------------------ reduce
 __device__ __forceinline__ double warp_sum(double v) {
@@ -574,6 +575,7 @@ struct CCStack {
     CCc<T> lv[MAXLEV];
     int off[MAXLEV];     // element offsets of z_l; b_l follows z_l
     int nu1, nu2, ncoarse;
+    const T* dinv;       // inverse of the last level's operator (solved exactly), or null
 };
 
 template <typename T>
@@ -582,7 +584,22 @@ struct FEMStack {
     FEMc<T> lv[MAXLEV];
     int off[MAXLEV];     // z_l, then b_l, then r_l
     int nu1, nu2, ncoarse;
+    const T* dinv;       // inverse of the last level's operator (solved exactly), or null
 };
+
+/** z = inv b for the CTA's last level (N unknowns, inv row-major in global
+ * memory): warp w takes rows w, w + 32, ...; lanes split each row. */
+template <typename T>
+__device__ void cta_direct(const T* __restrict__ inv, int N, const T* b, T* z) {
+    const int lane = threadIdx.x & 31;
+    for (int r = threadIdx.x >> 5; r < N; r += blockDim.x >> 5) {
+        T s = 0;
+        for (int k = lane; k < N; k += 32) s += inv[size_t(r) * N + k] * b[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) z[r] = s;
+    }
+    __syncthreads();
+}
 
 /** Row loops of the CTA-resident levels: warp w takes rows w, w+nw, ...;
  * lanes take columns, so no index division is needed. */
@@ -662,10 +679,14 @@ __global__ void __launch_bounds__(CTA_THREADS) cc_cta_cycle(CCStack<T> st, const
         const CCc<T>& c = st.lv[st.nl - 1];
         T* z = sm + st.off[st.nl - 1];
         T* b = z + c.m * c.n;
-        int ns = st.nl > 1 ? st.ncoarse : st.nu1 + st.nu2;
-        for (int s = 0; s < ns; s++) {
-            cta_sweep(c, z, b, 0);
-            cta_sweep(c, z, b, 1);
+        if (st.dinv) {
+            cta_direct(st.dinv, c.m * c.n, b, z);
+        } else {
+            int ns = st.nl > 1 ? st.ncoarse : st.nu1 + st.nu2;
+            for (int s = 0; s < ns; s++) {
+                cta_sweep(c, z, b, 0);
+                cta_sweep(c, z, b, 1);
+            }
         }
     }
     for (int l = st.nl - 2; l >= 0; l--) {
@@ -735,9 +756,13 @@ __global__ void __launch_bounds__(CTA_THREADS) fem_cta_cycle(FEMStack<T> st, con
         const FEMc<T>& c = st.lv[st.nl - 1];
         T* z = sm + st.off[st.nl - 1];
         T* b = z + c.M * c.N;
-        int ns = st.nl > 1 ? st.ncoarse : st.nu1 + st.nu2;
-        for (int s = 0; s < ns; s++)
-            for (int q = 0; q < 4; q++) cta_sweep(c, z, b, q);
+        if (st.dinv) {
+            cta_direct(st.dinv, c.M * c.N, b, z);
+        } else {
+            int ns = st.nl > 1 ? st.ncoarse : st.nu1 + st.nu2;
+            for (int s = 0; s < ns; s++)
+                for (int q = 0; q < 4; q++) cta_sweep(c, z, b, q);
+        }
     }
     for (int l = st.nl - 2; l >= 0; l--) {
         const FEMc<T>& c = st.lv[l];
@@ -927,6 +952,11 @@ class MG {
     // levels whose arrays fit in this many bytes run in the single-CTA cycle
     // (autotuned per grid; at most CTA_SMEM_LIMIT)
     size_t cta_limit = CTA_SMEM_LIMIT;
+    // the first CTA-resident level with at most DIRECT_MAX unknowns is solved
+    // exactly with its inverse instead of by the coarser levels' smoothing
+    int dlev = -1;
+    double* dinv64 = nullptr;
+    float* dinv32 = nullptr;
     int nu1 = 2, nu2 = 2;
     double rtol = 1e-10;
     int max_it = 200;
@@ -945,6 +975,11 @@ class MG {
         if (ctl) cudaFree(ctl);
         ctl = nullptr;
         gen.release();
+        if (dinv64) cudaFree(dinv64);
+        if (dinv32) cudaFree(dinv32);
+        dinv64 = nullptr;
+        dinv32 = nullptr;
+        dlev = -1;
     }
 
     bool fem() const { return kind == VDI_MG_FEM; }
@@ -1168,6 +1203,7 @@ class MG {
         VDI_CUDA(fem_tile_attr<double>());
         VDI_CUDA(fem_tile_attr<float>());
         VDI_CUDA((fem_tile_attr<double, float>()));
+        VDI_TRY(setup_direct());
         return VDI_OK;
     }
 
@@ -1187,6 +1223,47 @@ class MG {
         a.rd = rd;
         a.ctl = ctl;
         return a;
+    }
+
+    const double* dinv(double*) const { return dinv64; }
+    const float* dinv(float*) const { return dinv32; }
+
+    /** The direct coarsest solve: the first CTA-resident level with at most
+     * DIRECT_MAX unknowns, its operator probed into a stencil and inverted. */
+    int setup_direct() {
+        if (smooth_tail || general) return VDI_OK;
+        int from = std::max(nmulti64, nmulti32);
+        for (int l = std::max(from, 0); l < nlev; l++)
+            if (size(l) <= DIRECT_MAX) {
+                dlev = l;
+                break;
+            }
+        if (dlev < 0) return VDI_OK;
+        const int ml = lv[dlev].m, nl = lv[dlev].n;
+        const long N = size(dlev);
+        double* S;
+        VDI_CUDA(cudaMalloc(&S, 9 * N * sizeof(double)));
+        const int d = dlev;
+        auto apply = [&](const double* z, double* y) -> int {
+            if (fem()) apply_k<double><<<nblk(N), 256>>>(femc<double>(d), z, y);
+            else apply_k<double><<<nblk(N), 256>>>(ccc<double>(d), z, y);
+            VDI_CUDA(cudaGetLastError());
+            return VDI_OK;
+        };
+        int st = probe_stencil(ml, nl, S, apply);
+        std::vector<double> X;
+        if (st == VDI_OK) st = stencil_inverse(S, ml, nl, X);
+        cudaFree(S);
+        if (st != VDI_OK) {
+            dlev = -1;
+            return st;
+        }
+        std::vector<float> Xf(X.begin(), X.end());
+        VDI_CUDA(cudaMalloc(&dinv64, X.size() * sizeof(double)));
+        VDI_CUDA(cudaMalloc(&dinv32, X.size() * sizeof(float)));
+        VDI_CUDA(cudaMemcpy(dinv64, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice));
+        VDI_CUDA(cudaMemcpy(dinv32, Xf.data(), Xf.size() * sizeof(float), cudaMemcpyHostToDevice));
+        return VDI_OK;
     }
 
     double* ztmp(int l, double*) { return t64[l]; }
@@ -1216,6 +1293,10 @@ class MG {
                     off += 3 * int(size(l + q));
                 }
                 st.nu1 = nu1; st.nu2 = nu2; st.ncoarse = ncoarse_sweeps();
+                if (dlev >= l && dinv(static_cast<T*>(nullptr))) {
+                    st.nl = dlev - l + 1;
+                    st.dinv = dinv(static_cast<T*>(nullptr));
+                }
                 fem_cta_cycle<T><<<1, CTA_THREADS, smem, s>>>(st, b, z, zero_init);
             } else {
                 CCStack<T> st{};
@@ -1227,6 +1308,10 @@ class MG {
                     off += 2 * int(size(l + q));
                 }
                 st.nu1 = nu1; st.nu2 = nu2; st.ncoarse = ncoarse_sweeps();
+                if (dlev >= l && dinv(static_cast<T*>(nullptr))) {
+                    st.nl = dlev - l + 1;
+                    st.dinv = dinv(static_cast<T*>(nullptr));
+                }
                 cc_cta_cycle<T><<<1, CTA_THREADS, smem, s>>>(st, b, z, zero_init);
             }
             VDI_CUDA(cudaGetLastError());
@@ -1534,7 +1619,43 @@ int mg_kernels_per_iteration(const MG* mg, int precision) {
 }
 
 int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, double* z, float* ms, double* bytes) {
-    if (mg->nmulti64 < 1 || iters < 1) return VDI_ERR_INVALID_ARGUMENT;
+    if (iters < 1 || which < 0 || which > 3) return VDI_ERR_INVALID_ARGUMENT;
+    if (which >= 2) {
+        // 2: whole FP64 V-cycles back to back (mg_test.cc:36-43 times the
+        // same); 3: the single-CTA coarse cycle alone
+        if (which == 3 && (mg->general || mg->nmulti64 < 1 || mg->smooth_tail)) return VDI_ERR_INVALID_ARGUMENT;
+        const int l = mg->nmulti64;
+        auto launch = [&]() -> int {
+            if (which == 2) return mg->vcycle64(s, b, z, 0, 0, 0);
+            return mg->vcycle<double>(s, l, mg->b64[l], mg->z64[l], l, mg->z64, mg->b64, mg->smem64, 1, 0, 0, 0);
+        };
+        VDI_TRY(mg->vcycle64(s, b, z, 0, 0, 0));
+        VDI_TRY(launch());
+        cudaEvent_t e0, e1;
+        VDI_CUDA(cudaEventCreate(&e0));
+        VDI_CUDA(cudaEventCreate(&e1));
+        VDI_CUDA(cudaEventRecord(e0, s));
+        int st = VDI_OK;
+        for (int k = 0; k < iters && st == VDI_OK; k++) st = launch();
+        VDI_CUDA(cudaEventRecord(e1, s));
+        VDI_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        VDI_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        VDI_TRY(st);
+        *ms = t / iters;
+        // canonical bytes of a V-cycle: per level, each smoothing sweep reads
+        // z and b and writes z, and the transfers move 4.5 words per point
+        double pts = 0;
+        if (mg->general)
+            for (int q = 0; q < mg->gen.nlev(); q++) pts += double(mg->gen.size(q));
+        else
+            for (int q = 0; q < mg->nlev; q++) pts += double(mg->size(q));
+        *bytes = which == 2 ? (3. * (mg->nu1 + mg->nu2) + 4.5) * 8 * pts : 0.;
+        return VDI_OK;
+    }
+    if (mg->nmulti64 < 1) return VDI_ERR_INVALID_ARGUMENT;
     cudaEvent_t e0, e1;
     VDI_CUDA(cudaEventCreate(&e0));
     VDI_CUDA(cudaEventCreate(&e1));

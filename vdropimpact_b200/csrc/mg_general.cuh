@@ -238,6 +238,80 @@ __global__ void gen_coarse_k(const double* __restrict__ inv, const double* __res
     }
 }
 
+/** The inverse (row-major, N = m n) of the operator given by nine stencil
+ * planes on the device, formed on the host by Gauss-Jordan elimination with
+ * partial pivoting; for the small coarsest levels only. */
+static int stencil_inverse(const double* d_S, int m, int n, std::vector<double>& X) {
+    const int N = m * n;
+    std::vector<double> Sc(9 * size_t(N));
+    VDI_CUDA(cudaMemcpy(Sc.data(), d_S, Sc.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<double> A(size_t(N) * N, 0.);
+    X.assign(size_t(N) * N, 0.);
+    for (int k = 0; k < N; k++) {
+        int j = k / m, i = k - j * m;
+        for (int d = 0; d < 9; d++) {
+            int dx = d % 3 - 1, dy = d / 3 - 1;
+            int ii = i + dx, jj = j + dy;
+            if (ii < 0 || ii >= m || jj < 0 || jj >= n) continue;
+            A[size_t(k) * N + ii + size_t(m) * jj] += Sc[size_t(d) * N + k];
+        }
+        X[size_t(k) * N + k] = 1.;
+    }
+    for (int c = 0; c < N; c++) {
+        int piv = c;
+        for (int r = c + 1; r < N; r++)
+            if (std::fabs(A[size_t(r) * N + c]) > std::fabs(A[size_t(piv) * N + c])) piv = r;
+        if (A[size_t(piv) * N + c] == 0) {
+            set_error("multigrid: singular coarsest operator (%d unknowns)", N);
+            return VDI_ERR_UNSUPPORTED_SIZE;
+        }
+        if (piv != c)
+            for (int q = 0; q < N; q++) {
+                std::swap(A[size_t(c) * N + q], A[size_t(piv) * N + q]);
+                std::swap(X[size_t(c) * N + q], X[size_t(piv) * N + q]);
+            }
+        const double d = 1. / A[size_t(c) * N + c];
+        for (int q = 0; q < N; q++) {
+            A[size_t(c) * N + q] *= d;
+            X[size_t(c) * N + q] *= d;
+        }
+        for (int r = 0; r < N; r++) {
+            if (r == c) continue;
+            const double f = A[size_t(r) * N + c];
+            if (f == 0) continue;
+            for (int q = 0; q < N; q++) {
+                A[size_t(r) * N + q] -= f * A[size_t(c) * N + q];
+                X[size_t(r) * N + q] -= f * X[size_t(c) * N + q];
+            }
+        }
+    }
+    return VDI_OK;
+}
+
+/** Nine stencil planes of an operator on an m x n grid, probed through
+ * apply(p, y) (y = A p) with the nine lattice vectors. */
+template <class APPLY>
+static int probe_stencil(int m, int n, double* d_S, APPLY apply) {
+    const long N = long(m) * n;
+    double *p, *y;
+    VDI_CUDA(cudaMalloc(&p, N * sizeof(double)));
+    VDI_CUDA(cudaMalloc(&y, N * sizeof(double)));
+    int st = VDI_OK;
+    const int nb = std::max(1, std::min(nblk(N), 4096));
+    for (int py = 0; py < 3 && st == VDI_OK; py++)
+        for (int px = 0; px < 3 && st == VDI_OK; px++) {
+            gen_probe_k<<<nb, 256>>>(p, m, n, px, py);
+            st = apply(p, y);
+            if (st == VDI_OK) gen_extract_k<<<nb, 256>>>(y, d_S, m, n, px, py);
+        }
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaFree(p);
+    cudaFree(y);
+    VDI_TRY(st);
+    VDI_CUDA(e);
+    return VDI_OK;
+}
+
 /** The general hierarchy of one system. */
 struct GenMG {
     std::vector<int> gm, gn;          // level sizes
@@ -289,66 +363,13 @@ struct GenMG {
             }
         }
         // level 0: nine probes of the operator
-        double *p, *y;
-        VDI_CUDA(cudaMalloc(&p, size(0) * sizeof(double)));
-        VDI_CUDA(cudaMalloc(&y, size(0) * sizeof(double)));
-        int st = VDI_OK;
-        const int nb = std::min(nblk(size(0)), 4096);
-        for (int py = 0; py < 3 && st == VDI_OK; py++)
-            for (int px = 0; px < 3 && st == VDI_OK; px++) {
-                gen_probe_k<<<nb, 256>>>(p, m, n, px, py);
-                st = apply(p, y);
-                if (st == VDI_OK) gen_extract_k<<<nb, 256>>>(y, S[0], m, n, px, py);
-            }
-        cudaFree(p);
-        cudaFree(y);
-        VDI_TRY(st);
+        VDI_TRY(probe_stencil(m, n, S[0], apply));
         for (int l = 1; l < nlev(); l++)
             gen_rap_k<<<std::min(nblk(size(l)), 4096), 256>>>(S[l - 1], gm[l - 1], gn[l - 1], S[l], gm[l], gn[l]);
         VDI_CUDA(cudaGetLastError());
         // coarsest inverse by Gauss-Jordan with partial pivoting
-        const int L = nlev() - 1, mc = gm[L];
-        std::vector<double> Sc(9 * size_t(N));
-        VDI_CUDA(cudaMemcpy(Sc.data(), S[L], Sc.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        std::vector<double> A(size_t(N) * N, 0.), X(size_t(N) * N, 0.);
-        for (int k = 0; k < N; k++) {
-            int j = k / mc, i = k - j * mc;
-            for (int d = 0; d < 9; d++) {
-                int dx = d % 3 - 1, dy = d / 3 - 1;
-                int ii = i + dx, jj = j + dy;
-                if (ii < 0 || ii >= mc || jj < 0 || jj >= gn[L]) continue;
-                A[size_t(k) * N + ii + size_t(mc) * jj] += Sc[size_t(d) * N + k];
-            }
-            X[size_t(k) * N + k] = 1.;
-        }
-        for (int c = 0; c < N; c++) {
-            int piv = c;
-            for (int r = c + 1; r < N; r++)
-                if (std::fabs(A[size_t(r) * N + c]) > std::fabs(A[size_t(piv) * N + c])) piv = r;
-            if (A[size_t(piv) * N + c] == 0) {
-                set_error("multigrid: singular coarsest operator (%d unknowns)", N);
-                return VDI_ERR_UNSUPPORTED_SIZE;
-            }
-            if (piv != c)
-                for (int q = 0; q < N; q++) {
-                    std::swap(A[size_t(c) * N + q], A[size_t(piv) * N + q]);
-                    std::swap(X[size_t(c) * N + q], X[size_t(piv) * N + q]);
-                }
-            const double d = 1. / A[size_t(c) * N + c];
-            for (int q = 0; q < N; q++) {
-                A[size_t(c) * N + q] *= d;
-                X[size_t(c) * N + q] *= d;
-            }
-            for (int r = 0; r < N; r++) {
-                if (r == c) continue;
-                const double f = A[size_t(r) * N + c];
-                if (f == 0) continue;
-                for (int q = 0; q < N; q++) {
-                    A[size_t(r) * N + q] -= f * A[size_t(c) * N + q];
-                    X[size_t(r) * N + q] -= f * X[size_t(c) * N + q];
-                }
-            }
-        }
+        std::vector<double> X;
+        VDI_TRY(stencil_inverse(S[nlev() - 1], gm[nlev() - 1], gn[nlev() - 1], X));
         VDI_CUDA(cudaMalloc(&inv, X.size() * sizeof(double)));
         VDI_CUDA(cudaMemcpy(inv, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice));
         return VDI_OK;
