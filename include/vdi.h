@@ -243,10 +243,16 @@ enum vdi_mg_kind {
     VDI_MG_MAC = 0,           /* mgs_mac.hh:25-50: m x n cells, 5-point */
     VDI_MG_FEM = 1,           /* mgs_fem.hh:42-57: m x n nodes, 9-point FE */
     VDI_MG_VISC_U = 2,        /* visco_impl.hh:28-53, horizontal_vel = true */
-    VDI_MG_VISC_V = 3         /* visco_impl.hh:28-53, horizontal_vel = false */
+    VDI_MG_VISC_V = 3,        /* visco_impl.hh:28-53, horizontal_vel = false */
+    VDI_MG_MAC_NEUMANN = 4    /* the MAC operator with a Neumann bottom as well: a pure
+                                 Neumann Poisson problem (no reference counterpart; the
+                                 reference's systems are all nonsingular). The solve
+                                 projects b onto zero mean (its compatibility condition),
+                                 stops on the projected residual and returns the
+                                 zero-mean solution. */
 };
 typedef struct vdi_mg vdi_mg;
-/* MAC: c1 = dx, c2 = dy (mgs_mac.cc:23-27). FEM: c1 = dx, c2 = dy
+/* MAC (and MAC_NEUMANN): c1 = dx, c2 = dy (mgs_mac.cc:23-27). FEM: c1 = dx, c2 = dy
  * (mgs_fem.cc:26-30). VISC: c1 = vfx, c2 = vfy, x_sym as visco_impl. */
 int vdi_mg_create(int kind, int m, int n, double c1, double c2, int x_sym, void* stream, vdi_mg** out);
 int vdi_mg_destroy(vdi_mg* mg);

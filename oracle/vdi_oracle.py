@@ -187,13 +187,15 @@ def _assemble(m, n, diag, left, right, down, up, dl=None, dr=None, ul=None, ur=N
                          shape=(m * n, m * n))
 
 
-def mac_matrix(m, n, xxsp, yysp):
+def mac_matrix(m, n, xxsp, yysp, neumann_bottom=False):
     """mgs_mac.hh:33-48: cell-centred 5-point Laplacian, Neumann on the left,
-    right and top, Dirichlet (ghost reflection, -3*yysp) on the bottom."""
+    right and top, Dirichlet (ghost reflection, -3*yysp) on the bottom; with
+    neumann_bottom the bottom is Neumann too (the pure-Neumann variant, which
+    the reference does not have)."""
     i = np.arange(m)[None, :].repeat(n, 0)
     j = np.arange(n)[:, None].repeat(m, 1)
     diag = np.where((i > 0) & (i < m - 1), -2 * xxsp, -xxsp) + \
-        np.where(j == 0, -3 * yysp, np.where(j < n - 1, -2 * yysp, -yysp))
+        np.where(j == 0, (-1 if neumann_bottom else -3) * yysp, np.where(j < n - 1, -2 * yysp, -yysp))
     left = np.where(i > 0, xxsp, 0.); right = np.where(i < m - 1, xxsp, 0.)
     down = np.where(j > 0, yysp, 0.); up = np.where(j < n - 1, yysp, 0.)
     return _assemble(m, n, diag, left, right, down, up)

@@ -267,3 +267,51 @@ def test_general_vcycle_count_comparable(V, monkeypatch):
     g.b.copy_(b)
     v_gen, _ = g.solve_v_cycle(rtol=1e-10)
     assert v_gen <= v_fast + 4, (v_gen, v_fast)
+
+
+# ------------------------------------------------------- pure Neumann
+def _neumann_exact(m, n, dx, dy, b):
+    """The zero-mean solution of the singular system, from the bordered
+    matrix [[A, 1], [1^T, 0]] and the projected source."""
+    import scipy.sparse as sp
+    A = sp.csr_matrix(vo.mac_matrix(m, n, 1. / (dx * dx), 1. / (dy * dy), neumann_bottom=True))
+    one = sp.csr_matrix(np.ones((m * n, 1)))
+    K = sp.bmat([[A, one], [one.T, None]]).tocsc()
+    rhs = np.concatenate([b - b.mean(), [0.]])
+    return vo.DirectSolver(K).solve(rhs)[:-1], A
+
+
+@pytest.mark.parametrize("m,n", [(256, 128), (512, 256), (200, 100)])
+def test_mac_neumann_matches_exact(V, m, n):
+    """The source is given a nonzero mean on purpose: the solve projects it
+    out (the compatibility reduction) and returns the zero-mean solution."""
+    torch = _torch()
+    dx = 1. / m
+    b = gaussians_rhs(m, n, seed=21) + 0.37
+    zx, A = _neumann_exact(m, n, dx, dx, b)
+    s = V.MgsMacNeumann(m, n, dx, dx)
+    s.b.copy_(torch.from_numpy(b))
+    v, rel = s.solve_v_cycle(rtol=1e-10)
+    z = s.z.cpu().numpy()
+    bp = b - b.mean()
+    assert np.linalg.norm(bp - A @ z) / np.linalg.norm(bp) <= 1e-10 * (1 + 1e-6)
+    assert abs(z.mean()) <= 1e-12 * np.abs(z).max()
+    assert v <= 30, v
+    assert _rel(z, zx) < 1e-7
+
+
+def test_mac_neumann_config2_size(V):
+    """2048x1024, the single-projection workload's size: residual of the
+    projected source and the zero mean, checked on the device."""
+    torch = _torch()
+    m, n = 2048, 1024
+    dx = 1. / m
+    b = torch.from_numpy(gaussians_rhs(m, n, seed=5) + 1.5).cuda()
+    s = V.MgsMacNeumann(m, n, dx, dx)
+    s.b.copy_(b)
+    v, rel = s.solve_v_cycle(rtol=1e-10)
+    bp = b - b.mean()
+    r = bp - s.apply()
+    assert float(torch.linalg.norm(r) / torch.linalg.norm(bp)) <= 1e-10 * (1 + 1e-6)
+    assert abs(float(s.z.mean())) <= 1e-12 * float(s.z.abs().max())
+    assert v <= 30, v

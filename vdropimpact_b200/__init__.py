@@ -23,7 +23,7 @@ from . import _abi
 from ._abi import (VDI_MG_FP64, VDI_MG_MIXED, VDI_GUESS_EXTRAPOLATE, VDI_GUESS_LEARNED, VDI_MG_MAC,
                    VDI_MG_FEM, VDI_MG_VISC_U, VDI_MG_VISC_V, VdiError, check, lib)
 
-__all__ = ["Fluid2D", "MgsMac", "MgsFem", "ViscoImpl", "TriSolve", "VdiError", "params_from_cfg",
+__all__ = ["Fluid2D", "MgsMac", "MgsMacNeumann", "MgsFem", "ViscoImpl", "TriSolve", "VdiError", "params_from_cfg",
            "VDI_MG_FP64", "VDI_MG_MIXED", "VDI_GUESS_EXTRAPOLATE", "VDI_GUESS_LEARNED"]
 
 _PREC = {"fp64": VDI_MG_FP64, "mixed": VDI_MG_MIXED, "hybrid": _abi.VDI_MG_HYBRID, VDI_MG_FP64: VDI_MG_FP64,
@@ -412,6 +412,17 @@ class _MgSystem:
 class MgsMac(_MgSystem):
     """mgs_mac(int m,int n,double dx,double dy,double* b) (mgs_mac.cc:23-27)."""
     kind = VDI_MG_MAC
+
+    def __init__(self, m, n, dx, dy, stream=None):
+        super().__init__(m, n, dx, dy, False, stream)
+
+
+class MgsMacNeumann(_MgSystem):
+    """The MAC operator with Neumann conditions on all four sides (a pure
+    Neumann pressure Poisson problem, which the reference does not have): the
+    solve removes the source's mean (its compatibility condition) and returns
+    the zero-mean solution."""
+    kind = _abi.VDI_MG_MAC_NEUMANN
 
     def __init__(self, m, n, dx, dy, stream=None):
         super().__init__(m, n, dx, dy, False, stream)

@@ -39,6 +39,7 @@ VDI_MG_MAC = 0
 VDI_MG_FEM = 1
 VDI_MG_VISC_U = 2
 VDI_MG_VISC_V = 3
+VDI_MG_MAC_NEUMANN = 4
 
 
 class VdiParams(C.Structure):

@@ -925,6 +925,21 @@ static cudaError_t cc_tile_attr() {
     return cudaFuncSetAttribute(cc_tile<T, 1, 2, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
 }
 
+/** *out = mean of x (deterministic grid reduction in FP64). */
+__global__ void mean_k(const double* __restrict__ x, long N, Reduce rd, double* out) {
+    double s = 0;
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < N; k += long(gridDim.x) * blockDim.x) s += x[k];
+    s = block_sum(s);
+    double total;
+    if (grid_sum(s, rd, &total) && threadIdx.x == 0) *out = total / double(N);
+}
+
+__global__ void sub_mean_k(const double* src, double* dst, long N, const double* __restrict__ mean) {
+    const double mu = *mean;
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < N; k += long(gridDim.x) * blockDim.x)
+        dst[k] = src[k] - mu;
+}
+
 #include "mg_general.cuh"
 
 class MG {
@@ -980,24 +995,36 @@ class MG {
         dinv64 = nullptr;
         dinv32 = nullptr;
         dlev = -1;
+        if (bproj) cudaFree(bproj);
+        if (dmean) cudaFree(dmean);
+        bproj = nullptr;
+        dmean = nullptr;
     }
 
     bool fem() const { return kind == VDI_MG_FEM; }
+    bool mac_like() const { return kind == VDI_MG_MAC || kind == VDI_MG_MAC_NEUMANN; }
+    /** The pure-Neumann variant: singular (constants), solved on the
+     * zero-mean part of the source, with a zero-mean solution. */
+    bool neumann() const { return kind == VDI_MG_MAC_NEUMANN; }
+    double* bproj = nullptr;   // the source minus its mean (Neumann variant)
+    double* dmean = nullptr;   // a mean computed on the device
+    /** The source the iterations use. */
+    const double* rhs(const double* b) const { return neumann() ? bproj : b; }
     long size(int l) const { return long(lv[l].m) * lv[l].n; }
 
     /** Diagonals and couplings of level l, matching the problem classes'
      * a_cc / mul_a (mgs_mac.hh:33-45, visco_impl.hh:36-46) with the level's
      * scaled coefficients. */
     void fill_cc(LevelD& L, double kx, double ky) {
-        L.ox = kind == VDI_MG_MAC ? kx : -kx;
-        L.oy = kind == VDI_MG_MAC ? ky : -ky;
+        L.ox = mac_like() ? kx : -kx;
+        L.oy = mac_like() ? ky : -ky;
         bool horiz = kind == VDI_MG_VISC_U;
         for (int a = 0; a < 3; a++)
             for (int b = 0; b < 3; b++) {
                 double v;
-                if (kind == VDI_MG_MAC) {
+                if (mac_like()) {
                     double xp = a == 1 ? -2 * kx : -kx;
-                    double yp = b == 0 ? -3 * ky : (b == 1 ? -2 * ky : -ky);
+                    double yp = b == 0 ? (neumann() ? -ky : -3 * ky) : (b == 1 ? -2 * ky : -ky);
                     v = xp + yp;
                 } else {
                     double yp = b == 0 ? ky : 2 * ky;
@@ -1010,8 +1037,8 @@ class MG {
                 }
                 L.d[a][b] = v;
             }
-        if (kind == VDI_MG_MAC) {
-            L.gL = 1; L.gR = 1; L.gD = -1; L.gU = 1;
+        if (mac_like()) {
+            L.gL = 1; L.gR = 1; L.gD = neumann() ? 1 : -1; L.gU = 1;
         } else {
             L.gL = x_sym ? (horiz ? -1 : 1) : 0;
             L.gR = 0; L.gD = 1; L.gU = 0;
@@ -1066,7 +1093,7 @@ class MG {
         if (!need) {
             const LevelD& C = lv.back();
             bool small = size(nlev - 1) <= 64;
-            bool weak = kind != VDI_MG_MAC && kind != VDI_MG_FEM && 2 * (std::fabs(C.ox) + std::fabs(C.oy)) < 0.25;
+            bool weak = !mac_like() && kind != VDI_MG_FEM && 2 * (std::fabs(C.ox) + std::fabs(C.oy)) < 0.25;
             need = !small && !weak;
         }
         if (!need) return VDI_OK;
@@ -1114,7 +1141,7 @@ class MG {
                 // The viscous operator I - vfx Dxx - vfy Dyy is close to the
                 // identity once 2(vfx+vfy) is small: Gauss-Seidel alone solves
                 // that level, and coarser levels add nothing.
-                if (kind != VDI_MG_MAC && lv.size() >= 2 && 2 * (kx + ky) < 0.25) break;
+                if (!mac_like() && lv.size() >= 2 && 2 * (kx + ky) < 0.25) break;
                 mm >>= 1; nn >>= 1;
                 kx *= 0.25; ky *= 0.25;
             }
@@ -1153,6 +1180,10 @@ class MG {
     }
 
     int alloc() {
+        if (neumann()) {
+            VDI_CUDA(cudaMalloc(&bproj, size(0) * sizeof(double)));
+            VDI_CUDA(cudaMalloc(&dmean, sizeof(double)));
+        }
         if (general) {
             VDI_TRY(reduce_alloc(rd, MAX_PARTIALS));
             VDI_CUDA(cudaMalloc(&ctl, sizeof(SolveCtl)));
@@ -1165,7 +1196,7 @@ class MG {
                 VDI_CUDA(cudaGetLastError());
                 return VDI_OK;
             };
-            VDI_TRY(gen.setup(m, n, apply));
+            VDI_TRY(gen.setup(m, n, apply, neumann()));
             VDI_CUDA(cudaDeviceSynchronize());
             return VDI_OK;
         }
@@ -1231,7 +1262,7 @@ class MG {
     /** The direct coarsest solve: the first CTA-resident level with at most
      * DIRECT_MAX unknowns, its operator probed into a stencil and inverted. */
     int setup_direct() {
-        if (smooth_tail || general) return VDI_OK;
+        if (smooth_tail || general || neumann()) return VDI_OK;
         int from = std::max(nmulti64, nmulti32);
         for (int l = std::max(from, 0); l < nlev; l++)
             if (size(l) <= DIRECT_MAX) {
@@ -1408,7 +1439,22 @@ class MG {
         return VDI_OK;
     }
 
+    /** The Neumann compatibility step: dst = src - mean(src), the mean a
+     * deterministic FP64 grid reduction. */
+    int remove_mean(cudaStream_t s, const double* src, double* dst) {
+        const long N = size(0);
+        int nb = rblocks(N);
+        mean_k<<<nb, 256, 0, s>>>(src, N, rd, dmean);
+        sub_mean_k<<<std::min(nblk(N), 4096), 256, 0, s>>>(src, dst, N, dmean);
+        VDI_CUDA(cudaGetLastError());
+        return VDI_OK;
+    }
+
     int enqueue_begin(cudaStream_t s, const double* b, double* z) {
+        if (neumann()) {
+            VDI_TRY(remove_mean(s, b, bproj));
+            b = bproj;
+        }
         int nb = rblocks(size(0));
         norm2_kernel<<<nb, 256, 0, s>>>(b, size(0), rd, ctl);
         zero_if_b_zero<<<std::min(nb, 1184), 256, 0, s>>>(z, size(0), ctl);
@@ -1456,7 +1502,7 @@ class MG {
 };
 
 int mg_create(int kind, int m, int n, double c1, double c2, int x_sym, MG** out) {
-    if (!out || m < 2 || n < 2 || kind < 0 || kind > 3) {
+    if (!out || m < 2 || n < 2 || kind < 0 || kind > 4) {
         set_error("mg_create: invalid arguments");
         return VDI_ERR_INVALID_ARGUMENT;
     }
@@ -1518,13 +1564,18 @@ int mg_solve(MG* mg, cudaStream_t s, const double* b, double* z, double rtol, in
              int* vcycles, double* rel_res) {
     if (rtol != mg->rtol || max_it != mg->max_it) VDI_TRY(mg->set_ctl_params(s, rtol, max_it));
     VDI_TRY(mg->enqueue_begin(s, b, z));
-    VDI_TRY(mg->enqueue_first_check(s, b, z, precision, 0, 0));
+    const double* bb = mg->rhs(b);
+    VDI_TRY(mg->enqueue_first_check(s, bb, z, precision, 0, 0));
     SolveCtl h{};
     while (true) {
         VDI_CUDA(cudaMemcpyAsync(&h, mg->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s));
         VDI_CUDA(cudaStreamSynchronize(s));
         if (h.done) break;
-        VDI_TRY(mg->enqueue_body(s, b, z, precision, 0, 0));
+        VDI_TRY(mg->enqueue_body(s, bb, z, precision, 0, 0));
+    }
+    if (mg->neumann()) {
+        VDI_TRY(mg->remove_mean(s, z, z));
+        VDI_CUDA(cudaStreamSynchronize(s));
     }
     if (vcycles) *vcycles = h.it;
     if (rel_res) *rel_res = h.bnorm2 > 0 ? std::sqrt(h.rnorm2 / h.bnorm2) : 0.;
@@ -1559,7 +1610,8 @@ int mg_record_graph_solve(MG* mg, cudaStream_t s, const double* b, double* z, in
     if (cs != cudaStreamCaptureStatusActive) return VDI_ERR_NOT_READY;
     cudaGraphConditionalHandle h;
     VDI_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    VDI_TRY(mg->enqueue_first_check(s, b, z, precision, 1, h));
+    const double* bb = mg->rhs(b);
+    VDI_TRY(mg->enqueue_first_check(s, bb, z, precision, 1, h));
     VDI_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps));
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
@@ -1577,12 +1629,13 @@ int mg_record_graph_solve(MG* mg, cudaStream_t s, const double* b, double* z, in
         cudaStreamDestroy(bs);
         VDI_CUDA(e);
     }
-    int st = mg->enqueue_body(bs, b, z, precision, 1, h);
+    int st = mg->enqueue_body(bs, bb, z, precision, 1, h);
     cudaGraph_t bodyOut;
     e = cudaStreamEndCapture(bs, &bodyOut);
     cudaStreamDestroy(bs);
     if (st != VDI_OK) return st;
     VDI_CUDA(e);
+    if (mg->neumann()) VDI_TRY(mg->remove_mean(s, z, z));
     return VDI_OK;
 }
 

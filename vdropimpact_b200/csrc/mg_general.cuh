@@ -241,7 +241,7 @@ __global__ void gen_coarse_k(const double* __restrict__ inv, const double* __res
 /** The inverse (row-major, N = m n) of the operator given by nine stencil
  * planes on the device, formed on the host by Gauss-Jordan elimination with
  * partial pivoting; for the small coarsest levels only. */
-static int stencil_inverse(const double* d_S, int m, int n, std::vector<double>& X) {
+static int stencil_inverse(const double* d_S, int m, int n, std::vector<double>& X, bool pin_mean = false) {
     const int N = m * n;
     std::vector<double> Sc(9 * size_t(N));
     VDI_CUDA(cudaMemcpy(Sc.data(), d_S, Sc.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -256,6 +256,11 @@ static int stencil_inverse(const double* d_S, int m, int n, std::vector<double>&
             A[size_t(k) * N + ii + size_t(m) * jj] += Sc[size_t(d) * N + k];
         }
         X[size_t(k) * N + k] = 1.;
+    }
+    if (pin_mean) {
+        // a singular Neumann operator (constants in its null space): the last
+        // equation, redundant for a consistent source, becomes "sum = 0"
+        for (int q = 0; q < N; q++) A[size_t(N - 1) * N + q] = 1.;
     }
     for (int c = 0; c < N; c++) {
         int piv = c;
@@ -285,6 +290,8 @@ static int stencil_inverse(const double* d_S, int m, int n, std::vector<double>&
             }
         }
     }
+    if (pin_mean)
+        for (int r = 0; r < N; r++) X[size_t(r) * N + N - 1] = 0.;   // the constraint's right-hand side is 0
     return VDI_OK;
 }
 
@@ -336,7 +343,7 @@ struct GenMG {
 
     /** Builds the hierarchy; apply(z, y) computes y = A z on level 0. */
     template <class APPLY>
-    int setup(int m, int n, APPLY apply) {
+    int setup(int m, int n, APPLY apply, bool pin_mean = false) {
         release();
         gm.push_back(m);
         gn.push_back(n);
@@ -369,7 +376,7 @@ struct GenMG {
         VDI_CUDA(cudaGetLastError());
         // coarsest inverse by Gauss-Jordan with partial pivoting
         std::vector<double> X;
-        VDI_TRY(stencil_inverse(S[nlev() - 1], gm[nlev() - 1], gn[nlev() - 1], X));
+        VDI_TRY(stencil_inverse(S[nlev() - 1], gm[nlev() - 1], gn[nlev() - 1], X, pin_mean));
         VDI_CUDA(cudaMalloc(&inv, X.size() * sizeof(double)));
         VDI_CUDA(cudaMemcpy(inv, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice));
         return VDI_OK;

@@ -808,7 +808,7 @@ int vdi_mg_create(int kind, int m, int n, double c1, double c2, int x_sym, void*
     vdi_mg* h = new vdi_mg();
     h->s = static_cast<cudaStream_t>(stream);
     double a = c1, b = c2;
-    if (kind == VDI_MG_MAC) {
+    if (kind == VDI_MG_MAC || kind == VDI_MG_MAC_NEUMANN) {
         // mgs_mac.cc:23-27 (test constructor): xxsp = 1/(dx*dx)
         a = 1. / (c1 * c1);
         b = 1. / (c2 * c2);
