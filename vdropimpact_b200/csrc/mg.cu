@@ -280,10 +280,112 @@ struct CCTile {
 /** MODE 0: NS sweeps from zin (or zero), residual, restriction to bc (skipped
  * when bc is null). MODE 1: zin + prolonged zc, NS sweeps, and optionally the
  * residual norm with the solve decision. Both write zout. */
+/** The colour phases of a cell-centred window held in Z/B (split by
+ * colour); par0 is the colour parity of the window origin (zx, zy). */
+template <typename T, int MODE, int NS>
+__device__ __forceinline__ void cc_window_phases(const CCc<T>& c, T* Z, const T* B, int par0, bool inner, int zx,
+                                                 int zy) {
+    using G = CCTile<T, NS>;
+    constexpr int CW = G::CW, CH = G::CH, KW = G::KW, K = G::K;
+    constexpr int NW = G::NW, RPW = CH / NW;
+    const int m = c.m, n = c.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int ph = 0; ph < K; ph++) {
+        const int color = MODE == 1 ? ((ph & 1) ^ 1) : (ph & 1);
+        T* Zc = Z + color * CH * KW;
+        const T* Zo = Z + (color ^ 1) * CH * KW;
+        const T* Bc = B + color * CH * KW;
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            const int jj = warp + q * NW;
+            if (jj < 1 || jj > CH - 2) continue;
+            const int p = (color ^ par0 ^ jj) & 1;
+            const int ii = 2 * lane + p;
+            if (ii == 0 || ii == CW - 1) continue;
+            const T* zo = Zo + jj * KW;
+            const T l = zo[lane - 1 + p], r = zo[lane + p];
+            const T d = Zo[(jj - 1) * KW + lane], u = Zo[(jj + 1) * KW + lane];
+            T* w = Zc + jj * KW + lane;
+            if (inner) {
+                *w = (Bc[jj * KW + lane] - (c.ox * (l + r) + c.oy * (d + u))) * c.invd[1][1];
+            } else {
+                const int i = zx + ii, j = zy + jj;
+                if (unsigned(i) >= unsigned(m) || unsigned(j) >= unsigned(n)) continue;
+                T xs = (i > 0 ? l : T(0)) + (i < m - 1 ? r : T(0));
+                T ys = (j > 0 ? d : T(0)) + (j < n - 1 ? u : T(0));
+                *w = (Bc[jj * KW + lane] - (c.ox * xs + c.oy * ys)) * c.invd[cls(i, m)][cls(j, n)];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/** The end of a window: its interior written to zout, and (PRE) the
+ * restricted residual written to bc or (POST with norm) the window's sum of
+ * squared residuals returned. */
+template <typename T, int MODE, int NS, typename TC>
+__device__ __forceinline__ double cc_window_epilogue(const CCc<T>& c, const TileArgs<T, TC>& a, const T* Z,
+                                                    const T* B, int par0, int x0, int y0, int zx, int zy) {
+    using G = CCTile<T, NS>;
+    constexpr int CH = G::CH, KW = G::KW, ZH = G::ZH, TX = G::TX, TY = G::TY;
+    constexpr int NW = G::NW;
+    const int m = c.m, n = c.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto zat = [&](int ii, int jj) -> T { return Z[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)]; };
+    auto resid = [&](int ii, int jj) -> T {
+        const int i = zx + ii, j = zy + jj;
+        T bv = B[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)];
+        T xs = (i > 0 ? zat(ii - 1, jj) : T(0)) + (i < m - 1 ? zat(ii + 1, jj) : T(0));
+        T ys = (j > 0 ? zat(ii, jj - 1) : T(0)) + (j < n - 1 ? zat(ii, jj + 1) : T(0));
+        return bv - c.d[cls(i, m)][cls(j, n)] * zat(ii, jj) - (c.ox * xs + c.oy * ys);
+    };
+    // interior back to global memory (coalesced by row)
+    for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
+        const int j = zy + jj;
+        if (j >= n) break;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int ii = ZH + lane + 32 * h;
+            const int i = zx + ii;
+            if (ii < ZH + TX && i < m) a.zout[i + m * j] = zat(ii, jj);
+        }
+    }
+    double s = 0;
+    if (MODE == 0) {
+        if (a.bc) {
+            const int mc = m >> 1, nc = n >> 1;
+            constexpr int CX = TX / 2, CY = TY / 2;
+            for (int t = threadIdx.x; t < CX * CY; t += G::NT) {
+                const int q = t / CX;
+                const int I = x0 / 2 + (t - q * CX), J = y0 / 2 + q;
+                if (I >= mc || J >= nc) continue;
+                const int ii = 2 * I - zx, jj = 2 * J - zy;
+                T r = resid(ii, jj) + resid(ii + 1, jj) + resid(ii, jj + 1) + resid(ii + 1, jj + 1);
+                a.bc[I + mc * J] = TC(T(0.25) * r);
+            }
+        }
+    } else if (a.norm) {
+        for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
+            const int j = zy + jj;
+            if (j >= n) break;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int ii = ZH + lane + 32 * h;
+                if (ii < ZH + TX && zx + ii < m) {
+                    double r = double(resid(ii, jj));
+                    s += r * r;
+                }
+            }
+        }
+    }
+    return s;
+}
+
 template <typename T, int MODE, int NS, typename TC = T>
 __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<T, TC> a) {
     using G = CCTile<T, NS>;
-    constexpr int CW = G::CW, CH = G::CH, KW = G::KW, ZH = G::ZH, TX = G::TX, TY = G::TY, K = G::K;
+    constexpr int CW = G::CW, CH = G::CH, KW = G::KW, ZH = G::ZH, TX = G::TX, TY = G::TY;
     constexpr int NW = G::NW, RPW = CH / NW;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* Z = reinterpret_cast<T*>(sm_raw);
@@ -323,83 +425,9 @@ __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<
         }
     }
     __syncthreads();
-    // ---- colour phases
-#pragma unroll
-    for (int ph = 0; ph < K; ph++) {
-        const int color = MODE == 1 ? ((ph & 1) ^ 1) : (ph & 1);
-        T* Zc = Z + color * CH * KW;
-        const T* Zo = Z + (color ^ 1) * CH * KW;
-        const T* Bc = B + color * CH * KW;
-#pragma unroll
-        for (int q = 0; q < RPW; q++) {
-            const int jj = warp + q * NW;
-            if (jj < 1 || jj > CH - 2) continue;
-            const int p = (color ^ par0 ^ jj) & 1;
-            const int ii = 2 * lane + p;
-            if (ii == 0 || ii == CW - 1) continue;
-            const T* zo = Zo + jj * KW;
-            const T l = zo[lane - 1 + p], r = zo[lane + p];
-            const T d = Zo[(jj - 1) * KW + lane], u = Zo[(jj + 1) * KW + lane];
-            T* w = Zc + jj * KW + lane;
-            if (inner) {
-                *w = (Bc[jj * KW + lane] - (c.ox * (l + r) + c.oy * (d + u))) * c.invd[1][1];
-            } else {
-                const int i = zx + ii, j = zy + jj;
-                if (unsigned(i) >= unsigned(m) || unsigned(j) >= unsigned(n)) continue;
-                T xs = (i > 0 ? l : T(0)) + (i < m - 1 ? r : T(0));
-                T ys = (j > 0 ? d : T(0)) + (j < n - 1 ? u : T(0));
-                *w = (Bc[jj * KW + lane] - (c.ox * xs + c.oy * ys)) * c.invd[cls(i, m)][cls(j, n)];
-            }
-        }
-        __syncthreads();
-    }
-    // ---- epilogue helpers over window coordinates
-    auto zat = [&](int ii, int jj) -> T { return Z[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)]; };
-    auto resid = [&](int ii, int jj) -> T {
-        const int i = zx + ii, j = zy + jj;
-        T bv = B[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)];
-        T xs = (i > 0 ? zat(ii - 1, jj) : T(0)) + (i < m - 1 ? zat(ii + 1, jj) : T(0));
-        T ys = (j > 0 ? zat(ii, jj - 1) : T(0)) + (j < n - 1 ? zat(ii, jj + 1) : T(0));
-        return bv - c.d[cls(i, m)][cls(j, n)] * zat(ii, jj) - (c.ox * xs + c.oy * ys);
-    };
-    // interior back to global memory (coalesced by row)
-    for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
-        const int j = zy + jj;
-        if (j >= n) break;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int ii = ZH + lane + 32 * h;
-            const int i = zx + ii;
-            if (ii < ZH + TX && i < m) a.zout[i + m * j] = zat(ii, jj);
-        }
-    }
-    if (MODE == 0) {
-        if (a.bc) {
-            const int mc = m >> 1, nc = n >> 1;
-            constexpr int CX = TX / 2, CY = TY / 2;
-            for (int t = threadIdx.x; t < CX * CY; t += G::NT) {
-                const int q = t / CX;
-                const int I = x0 / 2 + (t - q * CX), J = y0 / 2 + q;
-                if (I >= mc || J >= nc) continue;
-                const int ii = 2 * I - zx, jj = 2 * J - zy;
-                T s = resid(ii, jj) + resid(ii + 1, jj) + resid(ii, jj + 1) + resid(ii + 1, jj + 1);
-                a.bc[I + mc * J] = TC(T(0.25) * s);
-            }
-        }
-    } else if (a.norm) {
-        double s = 0;
-        for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
-            const int j = zy + jj;
-            if (j >= n) break;
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int ii = ZH + lane + 32 * h;
-                if (ii < ZH + TX && zx + ii < m) {
-                    double r = double(resid(ii, jj));
-                    s += r * r;
-                }
-            }
-        }
+    cc_window_phases<T, MODE, NS>(c, Z, B, par0, inner, zx, zy);
+    double s = cc_window_epilogue<T, MODE, NS, TC>(c, a, Z, B, par0, x0, y0, zx, zy);
+    if (MODE == 1 && a.norm) {
         s = block_sum(s);
         double total;
         if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
@@ -921,8 +949,9 @@ static cudaError_t cc_tile_attr() {
     using G = CCTile<T, 2>;
     cudaError_t e = cudaFuncSetAttribute(cc_tile<T, 0, 2, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(G::smem));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(cc_tile<T, 1, 2, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(cc_tile<T, 1, 2, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem));
+    return e;
 }
 
 /** *out = mean of x (deterministic grid reduction in FP64). */
