@@ -68,6 +68,8 @@ struct vdi_sim {
     double* unet_r = nullptr;      // residual of the extrapolated guess (m x n)
     double* unet_norm = nullptr;   // its 2-norm
     float *unet_in = nullptr, *unet_out = nullptr;
+    // advection stages as one fused kernel (VDI_FUSED_ADVECT=0: four kernels)
+    bool fused_advect = true;
     // lift-off search (tt_analysis.cc:97-171) after every step
     LiftoffCfg lcfg{};
     LiftoffState* d_lift = nullptr;
@@ -123,11 +125,19 @@ int enqueue_step(vdi_sim* S, double dt) {
     if (S->lcfg.mode != VDI_LIFTOFF_OFF)
         VDI_TRY(liftoff_launch(S->s_gas, S->gas.h, S->lcfg, S->d_lift, S->d_lhist, S->lcap, dt));
     VDI_CUDA(cudaEventRecord(S->ev_gas, S->s_gas));
-    VDI_TRY(launch_stage1(s, g, S->f, dt));
-    VDI_TRY(launch_stage2(s, g, S->f));
-    VDI_TRY(launch_stage34(s, g, S->f, dt));
-    VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
-    VDI_TRY(launch_stage5_src(s, g, S->f, S->gas, dt, S->src_mac));
+    if (S->fused_advect) {
+        // stages 1-5 in one kernel, concurrent with the gas layer; the
+        // source's bottom-row term follows once the gas layer has finished
+        VDI_TRY(launch_advect(s, g, S->f, dt, S->src_mac));
+        VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
+        VDI_TRY(launch_mac_src_bottom(s, g, S->gas, dt, S->src_mac));
+    } else {
+        VDI_TRY(launch_stage1(s, g, S->f, dt));
+        VDI_TRY(launch_stage2(s, g, S->f));
+        VDI_TRY(launch_stage34(s, g, S->f, dt));
+        VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
+        VDI_TRY(launch_stage5_src(s, g, S->f, S->gas, dt, S->src_mac));
+    }
     VDI_TRY(guess(S, s, SOLVER_MAC, S->q, S->q_prev, S->q_prev2, mn));
     if (S->prm.mg_guess == VDI_GUESS_LEARNED) {
         // the network corrects the extrapolated guess from its residual
@@ -408,6 +418,7 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     const vdi_params& P = S->prm;
     g.m = P.m; g.n = P.n; g.x_sym = P.x_sym; g.implicit_visc = P.implicit_visc;
     g.blk_x = 32; g.blk_y = 8;
+    if (const char* e = getenv("VDI_FUSED_ADVECT")) S->fused_advect = atoi(e) != 0;
     g.ax = P.ax; g.ay = P.ay; g.bx = P.bx; g.by = P.by;
     // fluid_2d.cc:15-17
     g.dx = (P.bx - P.ax) / P.m;
@@ -760,7 +771,7 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     // residual check; per solve-loop iteration the kernels of its V-cycle;
     // per step the lift-off search when it is on, and with the learned guess
     // the residual kernel and the network's correction.
-    long per_step = 11 + (S->prm.implicit_visc ? 1 : 0) + (S->lcfg.mode != VDI_LIFTOFF_OFF ? 1 : 0) +
+    long per_step = 11 - (S->fused_advect ? 2 : 0) + (S->prm.implicit_visc ? 1 : 0) + (S->lcfg.mode != VDI_LIFTOFF_OFF ? 1 : 0) +
                     (S->prm.mg_guess == VDI_GUESS_LEARNED ? 1 + unet_kernels_per_correction() : 0);
     long launches = S->steps * per_step;
     for (int k = 0; k < 4; k++) {

@@ -211,6 +211,202 @@ __global__ void k_stage5_src(Grid g, Fields f, Gas gs, double dt, double* __rest
     src[i + g.m * j] = s;
 }
 
+// ------------------------------------------------ fused stages 1 to 5
+// k_stage1, k_stage2, k_stage34 and k_stage5_src (fluid_2d.cc:105-232) as
+// one kernel: a CTA loads u, v and p around a TX x TY tile once and carries
+// the stages through shared memory, each stage on a region one cell smaller
+// than the previous one's (stage 1 on the tile grown by two cells left and
+// below and three right and above, stage 2 by two/two, stages 3-4 by one).
+// It writes only what the rest of the step reads: the final edge velocities
+// ul, vl, vd, ud (with the ghost edges at the right and top), the viscous
+// force fc0, fc1 and the MAC source. The source's bottom-row gas-pressure
+// term depends on the gas layer, which runs concurrently, so
+// k_mac_src_bottom adds it after the two streams join. Every value is
+// computed by the same expressions as in the four kernels, so the results
+// are bit-identical.
+namespace {
+constexpr int ADV_TX = 32, ADV_TY = 16, ADV_NT = ADV_TX * ADV_TY;
+constexpr int ADV_W = ADV_TX + 4, ADV_H = ADV_TY + 4, ADV_N = ADV_W * ADV_H;   // edge windows
+constexpr int ADV_UW = ADV_TX + 8, ADV_UH = ADV_TY + 8;                        // u, v window
+constexpr int ADV_PW = ADV_TX + 3, ADV_PH = ADV_TY + 3;                        // pressure nodes
+constexpr size_t ADV_SMEM = (size_t(16) * ADV_N + 2 * ADV_UW * ADV_UH + ADV_PW * ADV_PH) * sizeof(double);
+}  // namespace
+
+__global__ void __launch_bounds__(ADV_NT) k_advect(Grid g, Fields f, double dt, double* __restrict__ src) {
+    extern __shared__ __align__(16) double asm_[];
+    double* E = asm_;                                  // 8 edge sets of stages 1-2: ud vd ul vl ur vr uu vu
+    double* E2 = E + 8 * ADV_N;                        // 8 edge sets of stage 4
+    double* U = E2 + 8 * ADV_N;
+    double* Vv = U + ADV_UW * ADV_UH;
+    double* Pn = Vv + ADV_UW * ADV_UH;
+    double *sud = E, *svd = E + ADV_N, *sul = E + 2 * ADV_N, *svl = E + 3 * ADV_N, *sur = E + 4 * ADV_N,
+           *svr = E + 5 * ADV_N, *suu = E + 6 * ADV_N, *svu = E + 7 * ADV_N;
+    double *sud2 = E2, *svd2 = E2 + ADV_N, *sul2 = E2 + 2 * ADV_N, *svl2 = E2 + 3 * ADV_N, *sur2 = E2 + 4 * ADV_N,
+           *svr2 = E2 + 5 * ADV_N, *suu2 = E2 + 6 * ADV_N, *svu2 = E2 + 7 * ADV_N;
+    const int m = g.m, n = g.n, P = m + 4;
+    const int x0 = blockIdx.x * ADV_TX, y0 = blockIdx.y * ADV_TY;
+    const int ox = x0 - 2, oy = y0 - 2;                // window cell (0,0)
+    const int tid = threadIdx.x;
+    // u, v over cells [x0-4, x0+TX+3] x [y0-4, y0+TY+3], inside the ghost layers
+    for (int t = tid; t < ADV_UW * ADV_UH; t += ADV_NT) {
+        const int i = x0 - 4 + t % ADV_UW, j = y0 - 4 + t / ADV_UW;
+        const bool in = i >= -2 && i <= m + 1 && j >= -2 && j <= n + 1;
+        const int c = (j + 2) * P + i + 2;
+        U[t] = in ? f.u[c] : 0.;
+        Vv[t] = in ? f.v[c] : 0.;
+    }
+    for (int t = tid; t < ADV_PW * ADV_PH; t += ADV_NT) {
+        const int i = x0 - 1 + t % ADV_PW, j = y0 - 1 + t / ADV_PW;
+        const bool in = i >= -2 && i <= m + 1 && j >= -2 && j <= n + 1;
+        Pn[t] = in ? f.p[(j + 2) * P + i + 2] : 0.;
+    }
+    __syncthreads();
+    auto uat = [&](int i, int j) { return U[(j - y0 + 4) * ADV_UW + (i - x0 + 4)]; };
+    auto vat = [&](int i, int j) { return Vv[(j - y0 + 4) * ADV_UW + (i - x0 + 4)]; };
+    auto pat = [&](int i, int j) { return Pn[(j - y0 + 1) * ADV_PW + (i - x0 + 1)]; };
+    // ---- stage 1 (k_stage1) on window cells [0, W) x [0, H)
+    for (int t = tid; t < ADV_N; t += ADV_NT) {
+        const int a = t % ADV_W, b = t / ADV_W, i = ox + a, j = oy + b;
+        if (i < 0 || i >= m || j < 0 || j >= n) continue;
+        double uc = uat(i, j), vc = vat(i, j);
+        double uy = g.ysp * mono_diff(uat(i, j - 2), uat(i, j - 1), uc, uat(i, j + 1), uat(i, j + 2));
+        double vy = g.ysp * mono_diff(vat(i, j - 2), vat(i, j - 1), vc, vat(i, j + 1), vat(i, j + 2));
+        double ux = g.xsp * mono_diff(uat(i - 2, j), uat(i - 1, j), uc, uat(i + 1, j), uat(i + 2, j));
+        double vx = g.xsp * mono_diff(vat(i - 2, j), vat(i - 1, j), vc, vat(i + 1, j), vat(i + 2, j));
+        sud[t] = uc - 0.5 * (g.dy + dt * vc) * uy;
+        svd[t] = vc - 0.5 * (g.dy + dt * vc) * vy;
+        sul[t] = (g.x_sym && i == 0) ? 0. : uc - 0.5 * (g.dx + dt * uc) * ux;
+        svl[t] = vc - 0.5 * (g.dx + dt * uc) * vx;
+        sur[t] = uc + 0.5 * (g.dx - dt * uc) * ux;
+        svr[t] = vc + 0.5 * (g.dx - dt * uc) * vx;
+        suu[t] = uc + 0.5 * (g.dy - dt * vc) * uy;
+        svu[t] = vc + 0.5 * (g.dy - dt * vc) * vy;
+    }
+    __syncthreads();
+    // ---- stage 2 (k_stage2) on window cells [0, W-1) x [0, H-1)
+    for (int t = tid; t < ADV_N; t += ADV_NT) {
+        const int a = t % ADV_W, b = t / ADV_W, i = ox + a, j = oy + b;
+        if (a >= ADV_W - 1 || b >= ADV_H - 1 || i < 0 || i >= m || j < 0 || j >= n) continue;
+        if (i < m - 1) {
+            double u0 = sur[t], u1 = sul[t + 1], v1 = svl[t + 1];
+            godunov_set_tang(u0, u1, svr[t], v1);
+            sur[t] = u0; sul[t + 1] = u1; svl[t + 1] = v1;
+            if (i == 0) sur[t - 1] = sul[t];
+        } else {
+            sul[t + 1] = sur[t];
+            svl[t + 1] = svr[t];
+        }
+        if (j < n - 1) {
+            double u0 = svu[t], u1 = svd[t + ADV_W], v1 = sud[t + ADV_W];
+            godunov_set_tang(u0, u1, suu[t], v1);
+            svu[t] = u0; svd[t + ADV_W] = u1; sud[t + ADV_W] = v1;
+            if (j == 0) svu[t - ADV_W] = svd[t];
+        } else {
+            svd[t + ADV_W] = svu[t];
+            sud[t + ADV_W] = suu[t];
+        }
+    }
+    __syncthreads();
+    // ---- stages 3-4 (k_stage34) on window cells [1, W-1) x [1, H-1)
+    for (int t = tid; t < ADV_N; t += ADV_NT) {
+        const int a = t % ADV_W, b = t / ADV_W, i = ox + a, j = oy + b;
+        if (a < 1 || a >= ADV_W - 1 || b < 1 || b >= ADV_H - 1 || i < 0 || i >= m || j < 0 || j >= n) continue;
+        double c0 = 0.5 * g.xsp * (sul[t + 1] + sul[t]) * (sur[t] - sur[t - 1]);
+        double c1 = 0.5 * g.xsp * (sul[t + 1] + sul[t]) * (svl[t + 1] - svl[t]);
+        double c2 = 0.5 * g.ysp * (svd[t + ADV_W] + svd[t]) * (sud[t + ADV_W] - sud[t]);
+        double c3 = 0.5 * g.ysp * (svd[t + ADV_W] + svd[t]) * (svu[t] - svu[t - ADV_W]);
+        double uc = uat(i, j), vc = vat(i, j);
+        double px = 0.5 * g.xsp * (pat(i + 1, j + 1) + pat(i + 1, j) - pat(i, j + 1) - pat(i, j));
+        double py = 0.5 * g.ysp * (pat(i + 1, j + 1) - pat(i + 1, j) + pat(i, j + 1) - pat(i, j));
+        double uyy = g.yysp * (uat(i, j - 1) - 2 * uc + uat(i, j + 1));
+        double vyy = g.yysp * (vat(i, j - 1) - 2 * vc + vat(i, j + 1));
+        double uxx = g.xxsp * (uat(i - 1, j) - 2 * uc + uat(i + 1, j));
+        double vxx = g.xxsp * (vat(i - 1, j) - 2 * vc + vat(i + 1, j));
+        double f_x = -px * g.rhoinv + g.viscfac * (uxx + uyy);
+        double f_y = -py * g.rhoinv + g.viscfac * (vxx + vyy);
+        // the slopes of stage 1, recomputed by the same expressions
+        double uy = g.ysp * mono_diff(uat(i, j - 2), uat(i, j - 1), uc, uat(i, j + 1), uat(i, j + 2));
+        double vy = g.ysp * mono_diff(vat(i, j - 2), vat(i, j - 1), vc, vat(i, j + 1), vat(i, j + 2));
+        double ux = g.xsp * mono_diff(uat(i - 2, j), uat(i - 1, j), uc, uat(i + 1, j), uat(i + 2, j));
+        double vx = g.xsp * mono_diff(vat(i - 2, j), vat(i - 1, j), vc, vat(i + 1, j), vat(i + 2, j));
+        sud2[t] = uc + 0.5 * (-g.dy * uy + dt * (-c0 - vc * uy + f_x));
+        svd2[t] = vc + 0.5 * (-g.dy * vy + dt * (-c1 - vc * vy + f_y));
+        sul2[t] = uc + 0.5 * (-g.dx * ux + dt * (-uc * ux - c2 + f_x));
+        svl2[t] = vc + 0.5 * (-g.dx * vx + dt * (-uc * vx - c3 + f_y));
+        sur2[t] = uc + 0.5 * (g.dx * ux + dt * (-uc * ux - c2 + f_x));
+        svr2[t] = vc + 0.5 * (g.dx * vx + dt * (-uc * vx - c3 + f_y));
+        suu2[t] = uc + 0.5 * (g.dy * uy + dt * (-c0 - vc * uy + f_x));
+        svu2[t] = vc + 0.5 * (g.dy * vy + dt * (-c1 - vc * vy + f_y));
+        if (a >= 2 && a < ADV_TX + 2 && b >= 2 && b < ADV_TY + 2) {
+            const int c = (j + 2) * P + i + 2;
+            f.fc0[c] = g.viscfac * (uxx + uyy);
+            f.fc1[c] = g.viscfac * (vxx + vyy);
+        }
+    }
+    __syncthreads();
+    // ---- stage 5 (k_stage5_src without the bottom gas term) on the tile
+    {
+        const int a = 2 + tid % ADV_TX, b = 2 + tid / ADV_TX, i = ox + a, j = oy + b;
+        if (i >= m || j >= n) return;
+        const int t = b * ADV_W + a;
+        const int c = (j + 2) * P + i + 2;
+        double ulL, vlL;
+        if (i == 0) {
+            ulL = g.x_sym ? 0. : sul2[t];
+            vlL = svl2[t];
+        } else {
+            ulL = sul2[t];
+            vlL = svl2[t];
+            godunov_set(sur2[t - 1], ulL, svr2[t - 1], vlL);
+        }
+        double ulR, vlR;
+        if (i < m - 1) {
+            ulR = sul2[t + 1];
+            vlR = svl2[t + 1];
+            godunov_set(sur2[t], ulR, svr2[t], vlR);
+        } else {
+            ulR = sur2[t];
+            vlR = svr2[t];
+            f.ul[c + 1] = ulR;
+            f.vl[c + 1] = vlR;
+        }
+        double vdB, udB;
+        if (j == 0) {
+            vdB = svd2[t];
+            udB = sud2[t];
+        } else {
+            vdB = svd2[t];
+            udB = sud2[t];
+            godunov_set(svu2[t - ADV_W], vdB, suu2[t - ADV_W], udB);
+        }
+        double vdT, udT;
+        if (j < n - 1) {
+            vdT = svd2[t + ADV_W];
+            udT = sud2[t + ADV_W];
+            godunov_set(svu2[t], vdT, suu2[t], udT);
+        } else {
+            vdT = svu2[t];
+            udT = suu2[t];
+            f.vd[c + P] = vdT;
+            f.ud[c + P] = udT;
+        }
+        f.ul[c] = ulL; f.vl[c] = vlL; f.vd[c] = vdB; f.ud[c] = udB;
+        src[i + g.m * j] = g.xsp * (ulR - ulL) + g.ysp * (vdT - vdB);
+    }
+}
+
+/** The bottom-row term of the MAC source (fluid_2d.cc:228-232), added once
+ * the gas layer has updated gp. */
+__global__ void k_mac_src_bottom(Grid g, Gas gs, double dt, double* __restrict__ src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.m) return;
+    const double macfac = 0.125 * g.rhoinv * dt;
+    double sbc = macfac * (gs.gp_old[i] + gs.gp_old[i + 1] + gs.gp[i] + gs.gp[i + 1]);
+    double s = src[i];
+    s -= 2 * g.yysp * sbc;
+    src[i] = s;
+}
+
 // ------------------------------------------- MAC correction + advection
 // fluid_2d.cc:236-261, with the corrected edge velocities formed on the fly.
 // Also advances the simulation time by dt/2 (fluid_2d.cc:251).
@@ -541,6 +737,21 @@ int launch_stage34(cudaStream_t s, const Grid& g, const Fields& f, double dt) {
 }
 int launch_stage5_src(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double dt, double* src) {
     k_stage5_src<<<cell_grid(g), cell_block(g), 0, s>>>(g, f, gs, dt, src);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_advect(cudaStream_t s, const Grid& g, const Fields& f, double dt, double* src) {
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_advect, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ADV_SMEM)) != cudaSuccess)
+            return VDI_ERR_CUDA;
+        attr = true;
+    }
+    dim3 grid((g.m + ADV_TX - 1) / ADV_TX, (g.n + ADV_TY - 1) / ADV_TY);
+    k_advect<<<grid, ADV_NT, ADV_SMEM, s>>>(g, f, dt, src);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_mac_src_bottom(cudaStream_t s, const Grid& g, const Gas& gs, double dt, double* src) {
+    k_mac_src_bottom<<<(g.m + 255) / 256, 256, 0, s>>>(g, gs, dt, src);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_mac_advect(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, const double* q, double dt,

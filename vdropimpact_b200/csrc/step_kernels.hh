@@ -66,6 +66,10 @@ int launch_stage1(cudaStream_t s, const Grid& g, const Fields& f, double dt);
 int launch_stage2(cudaStream_t s, const Grid& g, const Fields& f);
 int launch_stage34(cudaStream_t s, const Grid& g, const Fields& f, double dt);
 int launch_stage5_src(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double dt, double* src);
+/** Stages 1-5 of the advection in one kernel (all but the bottom-row gas
+ * term of the MAC source), and that term. */
+int launch_advect(cudaStream_t s, const Grid& g, const Fields& f, double dt, double* src);
+int launch_mac_src_bottom(cudaStream_t s, const Grid& g, const Gas& gs, double dt, double* src);
 int launch_mac_advect(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, const double* q, double dt,
                       double* d_time);
 int launch_inviscid_bc(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double dt);
