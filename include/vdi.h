@@ -175,6 +175,15 @@ typedef struct vdi_tune {
     int from_cache;           /* 1 when an earlier tuning of the same grid was reused */
 } vdi_tune;
 int vdi_sim_autotune(vdi_sim* sim, vdi_tune* out);
+/* Measurement helper (no reference counterpart): mean duration over iters
+ * back-to-back launches, with CUDA events on the simulation's stream, of one
+ * part of the step: which = 0 the fused advection kernel, 1 the four
+ * advection stage kernels, 2 the gas-layer update, 3 the lift-off analysis.
+ * The launches use the frame timestep and overwrite the step's intermediate
+ * arrays; which = 2 and 3 also advance the gas layer and the lift-off search,
+ * so the simulation should be re-initialised (or its state restored) after
+ * measuring. */
+int vdi_sim_profile(vdi_sim* sim, int which, int iters, float* ms);
 /* Applies a tuning (for example one saved from an earlier process). */
 int vdi_sim_set_tuning(vdi_sim* sim, const vdi_tune* tune);
 

@@ -200,6 +200,16 @@ class Fluid2D:
         check(lib().vdi_sim_autotune(self._h, C.byref(t)), "vdi_sim_autotune")
         return _tune_dict(t)
 
+    PROFILE = {"advect": 0, "advect_stages": 1, "gas": 2, "liftoff": 3}
+
+    def profile(self, part: str, iters: int = 20) -> float:
+        """Mean ms per launch of one part of the step (measurement only: it
+        overwrites intermediate arrays and, for "gas" and "liftoff", advances
+        the gas layer or the lift-off search)."""
+        ms = C.c_float()
+        check(lib().vdi_sim_profile(self._h, self.PROFILE[part], iters, C.byref(ms)), "vdi_sim_profile")
+        return ms.value
+
     LIFTOFF = {"off": 0, "smoothed": 1, "raw": 2}
 
     def liftoff_setup(self, mode="smoothed", every: int = 1, history: int = 0):

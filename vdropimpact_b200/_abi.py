@@ -120,6 +120,7 @@ _SIGS = [
     ("vdi_sim_device_field", C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(C.c_size_t)]),
     ("vdi_sim_autotune", C.c_int, [C.c_void_p, C.POINTER(VdiTune)]),
     ("vdi_sim_set_tuning", C.c_int, [C.c_void_p, C.POINTER(VdiTune)]),
+    ("vdi_sim_profile", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float)]),
     ("vdi_batch_create", C.c_int, [C.POINTER(VdiParams), C.c_int, C.POINTER(C.c_void_p)]),
     ("vdi_batch_destroy", C.c_int, [C.c_void_p]),
     ("vdi_batch_size", C.c_int, [C.c_void_p]),

@@ -1070,6 +1070,47 @@ int vdi_sim_autotune(vdi_sim* S, vdi_tune* out) {
     return VDI_OK;
 }
 
+int vdi_sim_profile(vdi_sim* S, int which, int iters, float* ms) {
+    if (!S || !ms || iters < 1 || which < 0 || which > 3) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    double dt;
+    VDI_TRY(vdi_sim_timestep_select(S, S->prm.t_end / S->prm.nframes, &dt, nullptr));
+    const Grid& g = S->g;
+    const int m = g.m;
+    auto launch = [&]() -> int {
+        switch (which) {
+            case 0: return launch_advect(S->s, g, S->f, dt, S->src_mac);
+            case 1:
+                VDI_TRY(launch_stage1(S->s, g, S->f, dt));
+                VDI_TRY(launch_stage2(S->s, g, S->f));
+                VDI_TRY(launch_stage34(S->s, g, S->f, dt));
+                return launch_stage5_src(S->s, g, S->f, S->gas, dt, S->src_mac);
+            case 2:
+                return launch_gas_update(S->s, S->gp, S->gas, S->f.u, S->f.v, m + 4, S->d_vframe, dt, S->d_time,
+                                         S->gas_work, S->d_err, S->d_gstats);
+            default:
+                return liftoff_launch(S->s, S->gas.h, S->lcfg, S->d_lift, S->d_lhist, S->lcap, dt);
+        }
+    };
+    if (which == 3 && S->lcfg.mode == VDI_LIFTOFF_OFF) return VDI_ERR_NOT_READY;
+    VDI_TRY(launch());
+    cudaEvent_t e0, e1;
+    VDI_CUDA(cudaEventCreate(&e0));
+    VDI_CUDA(cudaEventCreate(&e1));
+    VDI_CUDA(cudaEventRecord(e0, S->s));
+    int st = VDI_OK;
+    for (int k = 0; k < iters && st == VDI_OK; k++) st = launch();
+    VDI_CUDA(cudaEventRecord(e1, S->s));
+    VDI_CUDA(cudaEventSynchronize(e1));
+    float t = 0;
+    VDI_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    VDI_TRY(st);
+    *ms = t / iters;
+    return VDI_OK;
+}
+
 int vdi_sim_set_tuning(vdi_sim* S, const vdi_tune* t) {
     if (!S || !t || t->blk_x < 1 || t->blk_y < 1 || t->blk_x * t->blk_y > 1024) return VDI_ERR_INVALID_ARGUMENT;
     return apply_tuning(S, *t);

@@ -219,7 +219,9 @@ __global__ void k_stage5_src(Grid g, Fields f, Gas gs, double dt, double* __rest
 // below and three right and above, stage 2 by two/two, stages 3-4 by one).
 // It writes only what the rest of the step reads: the final edge velocities
 // ul, vl, vd, ud (with the ghost edges at the right and top), the viscous
-// force fc0, fc1 and the MAC source. The source's bottom-row gas-pressure
+// force fc0, fc1 and the MAC source. Stage 1 parks each cell's four limited
+// slopes in the stage-4 arrays, which stage 4 reads before it overwrites them.
+// The source's bottom-row gas-pressure
 // term depends on the gas layer, which runs concurrently, so
 // k_mac_src_bottom adds it after the two streams join. Every value is
 // computed by the same expressions as in the four kernels, so the results
@@ -273,6 +275,8 @@ __global__ void __launch_bounds__(ADV_NT) k_advect(Grid g, Fields f, double dt, 
         double vy = g.ysp * mono_diff(vat(i, j - 2), vat(i, j - 1), vc, vat(i, j + 1), vat(i, j + 2));
         double ux = g.xsp * mono_diff(uat(i - 2, j), uat(i - 1, j), uc, uat(i + 1, j), uat(i + 2, j));
         double vx = g.xsp * mono_diff(vat(i - 2, j), vat(i - 1, j), vc, vat(i + 1, j), vat(i + 2, j));
+        // the slopes wait for stage 4 in its own arrays, free until then
+        sul2[t] = ux; sud2[t] = uy; svl2[t] = vx; svd2[t] = vy;
         sud[t] = uc - 0.5 * (g.dy + dt * vc) * uy;
         svd[t] = vc - 0.5 * (g.dy + dt * vc) * vy;
         sul[t] = (g.x_sym && i == 0) ? 0. : uc - 0.5 * (g.dx + dt * uc) * ux;
@@ -324,11 +328,9 @@ __global__ void __launch_bounds__(ADV_NT) k_advect(Grid g, Fields f, double dt, 
         double vxx = g.xxsp * (vat(i - 1, j) - 2 * vc + vat(i + 1, j));
         double f_x = -px * g.rhoinv + g.viscfac * (uxx + uyy);
         double f_y = -py * g.rhoinv + g.viscfac * (vxx + vyy);
-        // the slopes of stage 1, recomputed by the same expressions
-        double uy = g.ysp * mono_diff(uat(i, j - 2), uat(i, j - 1), uc, uat(i, j + 1), uat(i, j + 2));
-        double vy = g.ysp * mono_diff(vat(i, j - 2), vat(i, j - 1), vc, vat(i, j + 1), vat(i, j + 2));
-        double ux = g.xsp * mono_diff(uat(i - 2, j), uat(i - 1, j), uc, uat(i + 1, j), uat(i + 2, j));
-        double vx = g.xsp * mono_diff(vat(i - 2, j), vat(i - 1, j), vc, vat(i + 1, j), vat(i + 2, j));
+        // this cell's slopes from stage 1, read before its stage-4 values
+        // overwrite them
+        double ux = sul2[t], uy = sud2[t], vx = svl2[t], vy = svd2[t];
         sud2[t] = uc + 0.5 * (-g.dy * uy + dt * (-c0 - vc * uy + f_x));
         svd2[t] = vc + 0.5 * (-g.dy * vy + dt * (-c1 - vc * vy + f_y));
         sul2[t] = uc + 0.5 * (-g.dx * ux + dt * (-uc * ux - c2 + f_x));
