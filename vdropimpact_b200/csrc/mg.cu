@@ -87,6 +87,38 @@ __device__ bool grid_sum(double blocksum, Reduce rd, double* total) {
     return true;
 }
 
+/** grid_sum of two values at once: partials k and nb + k (at most half of
+ * the partials array in blocks). */
+__device__ bool grid_sum2(double s1, double s2, Reduce rd, double* t1, double* t2) {
+    __shared__ int last;
+    const int nb = gridDim.x * gridDim.y;
+    const int bid = blockIdx.x + gridDim.x * blockIdx.y;
+    if (threadIdx.x == 0) {
+        rd.partials[bid] = s1;
+        rd.partials[nb + bid] = s2;
+        __threadfence();
+        unsigned t = atomicAdd(rd.counter, 1u);
+        last = (t == unsigned(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double a = 0, b = 0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        a += __ldcg(rd.partials + k);
+        b += __ldcg(rd.partials + nb + k);
+    }
+    a = block_sum(a);
+    __syncthreads();
+    b = block_sum(b);
+    if (threadIdx.x == 0) {
+        *t1 = a;
+        *t2 = b;
+        *rd.counter = 0;
+    }
+    return true;
+}
+
 int reduce_alloc(Reduce& r, int max_blocks) {
     r.max_blocks = max_blocks;
     VDI_CUDA(cudaMalloc(&r.partials, sizeof(double) * max_blocks));
@@ -836,6 +868,35 @@ __global__ void resid_norm_k(OP c, const T* __restrict__ z, const T* __restrict_
     if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
 }
 
+/** The start of a solve in one pass: ||b||^2 and ||b - A z0||^2, then the
+ * first decision (a zero source is done at once; zero_if_b_zero then sets z
+ * to zero). */
+template <typename T, class OP>
+__global__ void first_check_k(OP c, const T* __restrict__ z, const T* __restrict__ b, Reduce rd, SolveCtl* ctl,
+                              int use_cond, cudaGraphConditionalHandle h) {
+    double sb = 0, sr = 0;
+    const long tot = long(op_m(c)) * op_n(c);
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
+        int i, j;
+        grid_ij(c, k, i, j);
+        double bv = double(b[k]);
+        double r = double(op_resid(c, z + k, b[k], op_m(c), i, j));
+        sb += bv * bv;
+        sr += r * r;
+    }
+    sb = block_sum(sb);
+    __syncthreads();
+    sr = block_sum(sr);
+    double b2, r2;
+    if (grid_sum2(sb, sr, rd, &b2, &r2) && threadIdx.x == 0) {
+        ctl->bnorm2 = b2;
+        ctl->it = 0;
+        ctl->done = 0;
+        ctl->status = 0;
+        solve_decide(ctl, b2 == 0. ? 0. : r2, 0, use_cond, h);
+    }
+}
+
 /** FP64 residual of an FP64 iterate written as FP32 (a refinement step),
  * with its FP64 norm and the solve decision. */
 template <class OP>
@@ -1480,14 +1541,7 @@ class MG {
     }
 
     int enqueue_begin(cudaStream_t s, const double* b, double* z) {
-        if (neumann()) {
-            VDI_TRY(remove_mean(s, b, bproj));
-            b = bproj;
-        }
-        int nb = rblocks(size(0));
-        norm2_kernel<<<nb, 256, 0, s>>>(b, size(0), rd, ctl);
-        zero_if_b_zero<<<std::min(nb, 1184), 256, 0, s>>>(z, size(0), ctl);
-        VDI_CUDA(cudaGetLastError());
+        if (neumann()) VDI_TRY(remove_mean(s, b, bproj));
         return VDI_OK;
     }
 
@@ -1506,10 +1560,26 @@ class MG {
         return VDI_OK;
     }
 
-    int enqueue_first_check(cudaStream_t s, const double* b, const double* z, int precision, int use_cond,
+    int enqueue_first_check(cudaStream_t s, const double* b, double* z, int precision, int use_cond,
                             cudaGraphConditionalHandle h) {
-        if (precision == VDI_MG_MIXED && !general) return enqueue_resid32(s, b, z, 0, use_cond, h);
-        return enqueue_resid_norm(s, b, z, 0, use_cond, h);
+        const long N = size(0);
+        if (precision == VDI_MG_MIXED && !general) {
+            int nb = rblocks(N);
+            norm2_kernel<<<nb, 256, 0, s>>>(b, N, rd, ctl);
+            zero_if_b_zero<<<std::min(nb, 1184), 256, 0, s>>>(z, N, ctl);
+            VDI_CUDA(cudaGetLastError());
+            return enqueue_resid32(s, b, z, 0, use_cond, h);
+        }
+        int nb = std::max(1, std::min(MAX_PARTIALS / 2, nblk(N, 256)));
+        if (general)
+            first_check_k<double><<<nb, 256, 0, s>>>(gen.op(0), z, b, rd, ctl, use_cond, h);
+        else if (fem())
+            first_check_k<double><<<nb, 256, 0, s>>>(femc<double>(0), z, b, rd, ctl, use_cond, h);
+        else
+            first_check_k<double><<<nb, 256, 0, s>>>(ccc<double>(0), z, b, rd, ctl, use_cond, h);
+        zero_if_b_zero<<<std::min(nb, 1184), 256, 0, s>>>(z, N, ctl);
+        VDI_CUDA(cudaGetLastError());
+        return VDI_OK;
     }
 
     int set_ctl_params(cudaStream_t s, double rt, int mx) {

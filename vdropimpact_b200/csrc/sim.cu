@@ -767,8 +767,8 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     // launches: per step the gas-layer update, the four stencil stages, the
     // MAC correction, two boundary kernels, the FEM source, the velocity update
     // and the final boundary kernel (+1 viscous source when implicit), two
-    // kernels per initial guess; per solve two set-up kernels and the first
-    // residual check; per solve-loop iteration the kernels of its V-cycle;
+    // kernels per initial guess; per solve the start check; per solve-loop
+    // iteration the kernels of its V-cycle;
     // per step the lift-off search when it is on, and with the learned guess
     // the residual kernel and the network's correction.
     long per_step = 11 - (S->fused_advect ? 2 : 0) + (S->prm.implicit_visc ? 1 : 0) + (S->lcfg.mode != VDI_LIFTOFF_OFF ? 1 : 0) +
@@ -776,7 +776,11 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     long launches = S->steps * per_step;
     for (int k = 0; k < 4; k++) {
         if (!S->mg[k]) continue;
-        launches += out->solves[k] * (2 + 3) + out->vcycles[k] * mg_kernels_per_iteration(S->mg[k], S->prm.mg_precision);
+        // two guess kernels; the start check and the zeroing kernel (mixed
+        // precision: norm, zeroing and the refinement residual)
+        const int start = S->prm.mg_precision == VDI_MG_MIXED ? 3 : 2;
+        launches += out->solves[k] * (2 + start) +
+                    out->vcycles[k] * mg_kernels_per_iteration(S->mg[k], S->prm.mg_precision);
     }
     out->kernel_launches = launches;
     GasStats gs;
