@@ -134,11 +134,14 @@ def test_visc_solve(V, x_sym, horiz, prec):
     assert _rel(z, vo.DirectSolver(A).solve(b)) < 1e-9
 
 
-def test_zero_rhs_gives_zero(V):
-    torch = _torch()
-    s = V.MgsMac(64, 32, 0.1, 0.1)
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "hybrid"])
+@pytest.mark.parametrize("kind,m,n", [("mac", 64, 32), ("mac", 1024, 512), ("fem", 513, 257), ("mac", 135, 77)])
+def test_zero_rhs_gives_zero(V, kind, m, n, prec):
+    """A zero source is solved at once with z = 0, whatever z held, on one
+    block and on many, on the fixed and the Galerkin hierarchy."""
+    s = (V.MgsMac if kind == "mac" else V.MgsFem)(m, n, 0.1, 0.1)
     s.z.fill_(3.0)
-    v, rel = s.solve_v_cycle()
+    v, rel = s.solve_v_cycle(precision=prec)
     assert v == 0 and float(s.z.abs().max()) == 0.0
 
 

@@ -869,11 +869,13 @@ __global__ void resid_norm_k(OP c, const T* __restrict__ z, const T* __restrict_
 }
 
 /** The start of a solve in one pass: ||b||^2 and ||b - A z0||^2, then the
- * first decision (a zero source is done at once; zero_if_b_zero then sets z
- * to zero). */
+ * first decision. A zero source is done at once with z = 0 (the shim and
+ * this library agree on that convention): the last block, which every other
+ * block has finished reading z before, zeroes it. */
 template <typename T, class OP>
-__global__ void first_check_k(OP c, const T* __restrict__ z, const T* __restrict__ b, Reduce rd, SolveCtl* ctl,
+__global__ void first_check_k(OP c, T* __restrict__ z, const T* __restrict__ b, Reduce rd, SolveCtl* ctl,
                               int use_cond, cudaGraphConditionalHandle h) {
+    __shared__ int zero_src;
     double sb = 0, sr = 0;
     const long tot = long(op_m(c)) * op_n(c);
     for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
@@ -888,13 +890,18 @@ __global__ void first_check_k(OP c, const T* __restrict__ z, const T* __restrict
     __syncthreads();
     sr = block_sum(sr);
     double b2, r2;
-    if (grid_sum2(sb, sr, rd, &b2, &r2) && threadIdx.x == 0) {
+    if (!grid_sum2(sb, sr, rd, &b2, &r2)) return;
+    if (threadIdx.x == 0) {
         ctl->bnorm2 = b2;
         ctl->it = 0;
         ctl->done = 0;
         ctl->status = 0;
         solve_decide(ctl, b2 == 0. ? 0. : r2, 0, use_cond, h);
+        zero_src = b2 == 0.;
     }
+    __syncthreads();
+    if (zero_src)
+        for (long k = threadIdx.x; k < tot; k += blockDim.x) z[k] = T(0);
 }
 
 /** FP64 residual of an FP64 iterate written as FP32 (a refinement step),
@@ -1577,7 +1584,6 @@ class MG {
             first_check_k<double><<<nb, 256, 0, s>>>(femc<double>(0), z, b, rd, ctl, use_cond, h);
         else
             first_check_k<double><<<nb, 256, 0, s>>>(ccc<double>(0), z, b, rd, ctl, use_cond, h);
-        zero_if_b_zero<<<std::min(nb, 1184), 256, 0, s>>>(z, N, ctl);
         VDI_CUDA(cudaGetLastError());
         return VDI_OK;
     }

@@ -38,6 +38,7 @@ struct vdi_sim {
     cudaStream_t s = nullptr, s_gas = nullptr, s_vy = nullptr;
     bool own_stream = false;
     cudaEvent_t ev_fork = nullptr, ev_gas = nullptr, ev_vy = nullptr, ev_vy_done = nullptr;
+    cudaEvent_t ev_adv = nullptr, ev_side = nullptr;   // advection done; side-stream work done
     std::vector<double*> bufs;
     Fields f{};
     Gas gas{};
@@ -103,11 +104,10 @@ int update_visc(vdi_sim* S, double dt) {
 }
 
 /** mgs_common::initial_guess (mgs_common.cc:17-50) for one solver, or the
- * quadratic variant when the parameters ask for it. */
-int guess(vdi_sim* S, cudaStream_t s, int which, double* z, double* zp, double* zp2, int n) {
-    if (S->prm.mg_guess == VDI_GUESS_QUADRATIC || S->prm.mg_guess == VDI_GUESS_LEARNED)
-        return launch_guess2(s, z, zp, zp2, n, S->hist + which, S->d_time, S->d_err);
-    return launch_guess(s, z, zp, n, S->hist + which, S->d_time, S->d_err);
+ * quadratic variant when the parameters ask for it, at time *d_time + tadd. */
+int guess(vdi_sim* S, cudaStream_t s, int which, double* z, double* zp, double* zp2, int n, double tadd = 0.) {
+    const int quad = S->prm.mg_guess == VDI_GUESS_QUADRATIC || S->prm.mg_guess == VDI_GUESS_LEARNED;
+    return launch_guess(s, z, zp, zp2, n, S->hist + which, S->d_time, tadd, quad, S->d_err);
 }
 
 /** Enqueues one fluid_2d::step_forward(dt) (fluid_2d.cc:93-405). */
@@ -116,7 +116,16 @@ int enqueue_step(vdi_sim* S, double dt) {
     cudaStream_t s = S->s;
     const int m = g.m, n = g.n, mn = m * n, nf = (m + 1) * (n + 1);
     int prec = S->prm.mg_precision;
-    // gas layer on its own stream; it overlaps the advection stages
+    // The gas layer runs on its own stream, overlapping the advection. The
+    // same stream then takes the work that needs neither the advection's
+    // output nor the MAC solve, off the main stream's path:
+    //  - the MAC guess (it needs the clock advanced by the gas layer);
+    //  - once the advection has read the ghost cells, the far-field boundary
+    //    kernel (it writes only ghost velocities, which nothing before the
+    //    MAC correction reads, and the gas pressure);
+    //  - the FEM guess, at the time the MAC correction will set (tadd = dt/2).
+    // The main stream joins before the MAC correction, which advances the
+    // clock, so the FEM guess has read it by then.
     VDI_CUDA(cudaEventRecord(S->ev_fork, s));
     VDI_CUDA(cudaStreamWaitEvent(S->s_gas, S->ev_fork, 0));
     VDI_TRY(launch_gas_update(S->s_gas, S->gp, S->gas, S->f.u, S->f.v, m + 4, S->d_vframe, dt, S->d_time,
@@ -124,11 +133,13 @@ int enqueue_step(vdi_sim* S, double dt) {
     // h is final for this step once the gas layer has updated it
     if (S->lcfg.mode != VDI_LIFTOFF_OFF)
         VDI_TRY(liftoff_launch(S->s_gas, S->gas.h, S->lcfg, S->d_lift, S->d_lhist, S->lcap, dt));
+    VDI_TRY(guess(S, S->s_gas, SOLVER_MAC, S->q, S->q_prev, S->q_prev2, mn));
     VDI_CUDA(cudaEventRecord(S->ev_gas, S->s_gas));
     if (S->fused_advect) {
         // stages 1-5 in one kernel, concurrent with the gas layer; the
         // source's bottom-row term follows once the gas layer has finished
         VDI_TRY(launch_advect(s, g, S->f, dt, S->src_mac));
+        VDI_CUDA(cudaEventRecord(S->ev_adv, s));
         VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
         VDI_TRY(launch_mac_src_bottom(s, g, S->gas, dt, S->src_mac));
     } else {
@@ -137,8 +148,12 @@ int enqueue_step(vdi_sim* S, double dt) {
         VDI_TRY(launch_stage34(s, g, S->f, dt));
         VDI_CUDA(cudaStreamWaitEvent(s, S->ev_gas, 0));
         VDI_TRY(launch_stage5_src(s, g, S->f, S->gas, dt, S->src_mac));
+        VDI_CUDA(cudaEventRecord(S->ev_adv, s));
     }
-    VDI_TRY(guess(S, s, SOLVER_MAC, S->q, S->q_prev, S->q_prev2, mn));
+    VDI_CUDA(cudaStreamWaitEvent(S->s_gas, S->ev_adv, 0));
+    VDI_TRY(launch_inviscid_bc(S->s_gas, g, S->f, S->gas, dt));
+    VDI_TRY(guess(S, S->s_gas, SOLVER_FEM, S->zf, S->zf_prev, S->zf_prev2, nf, 0.5 * dt));
+    VDI_CUDA(cudaEventRecord(S->ev_side, S->s_gas));
     if (S->prm.mg_guess == VDI_GUESS_LEARNED) {
         // the network corrects the extrapolated guess from its residual
         if (!S->unet) {
@@ -150,8 +165,8 @@ int enqueue_step(vdi_sim* S, double dt) {
                              S->unet_in, S->unet_out));
     }
     VDI_TRY(mg_solve_device(S->mg[SOLVER_MAC], s, S->src_mac, S->q, prec));
+    VDI_CUDA(cudaStreamWaitEvent(s, S->ev_side, 0));
     VDI_TRY(launch_mac_advect(s, g, S->f, S->gas, S->q, dt, S->d_time));
-    VDI_TRY(launch_inviscid_bc(s, g, S->f, S->gas, dt));
     VDI_TRY(launch_viscous_bc(s, g, S->f, S->gas));
     CellView c0v, c1v;
     if (g.implicit_visc) {
@@ -179,7 +194,6 @@ int enqueue_step(vdi_sim* S, double dt) {
         c1v = CellView{S->f.fc1, m + 4, 2 * (m + 4) + 2};
     }
     VDI_TRY(launch_fem_rhs(s, g, S->f, S->gas, c0v, c1v, dt, S->fem_acc_edge, S->fem_acc_mid, S->src_fem));
-    VDI_TRY(guess(S, s, SOLVER_FEM, S->zf, S->zf_prev, S->zf_prev2, nf));
     VDI_TRY(mg_solve_device(S->mg[SOLVER_FEM], s, S->src_fem, S->zf, prec));
     VDI_TRY(launch_vel_update(s, g, S->f, c0v, c1v, S->zf, dt));
     VDI_TRY(launch_viscous_bc(s, g, S->f, S->gas));
@@ -450,7 +464,9 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
         cudaEventCreateWithFlags(&S->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&S->ev_gas, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&S->ev_vy, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&S->ev_vy_done, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&S->ev_vy_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_adv, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_side, cudaEventDisableTiming) != cudaSuccess)
         return fail(VDI_ERR_CUDA);
     size_t NG = ghosted(S);
     double** fptrs[] = {&S->f.u, &S->f.v, &S->f.p, &S->f.ux, &S->f.uy, &S->f.vx, &S->f.vy,
@@ -556,6 +572,8 @@ int vdi_sim_destroy(vdi_sim* S) {
     if (S->ev_gas) cudaEventDestroy(S->ev_gas);
     if (S->ev_vy) cudaEventDestroy(S->ev_vy);
     if (S->ev_vy_done) cudaEventDestroy(S->ev_vy_done);
+    if (S->ev_adv) cudaEventDestroy(S->ev_adv);
+    if (S->ev_side) cudaEventDestroy(S->ev_side);
     if (S->s_gas) cudaStreamDestroy(S->s_gas);
     if (S->s_vy) cudaStreamDestroy(S->s_vy);
     if (S->own_stream && S->s) cudaStreamDestroy(S->s);
@@ -766,9 +784,9 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     }
     // launches: per step the gas-layer update, the four stencil stages, the
     // MAC correction, two boundary kernels, the FEM source, the velocity update
-    // and the final boundary kernel (+1 viscous source when implicit), two
-    // kernels per initial guess; per solve the start check; per solve-loop
-    // iteration the kernels of its V-cycle;
+    // and the final boundary kernel (+1 viscous source when implicit); per
+    // solve the initial guess and the start check; per solve-loop iteration
+    // the kernels of its V-cycle;
     // per step the lift-off search when it is on, and with the learned guess
     // the residual kernel and the network's correction.
     long per_step = 11 - (S->fused_advect ? 2 : 0) + (S->prm.implicit_visc ? 1 : 0) + (S->lcfg.mode != VDI_LIFTOFF_OFF ? 1 : 0) +
@@ -776,10 +794,10 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     long launches = S->steps * per_step;
     for (int k = 0; k < 4; k++) {
         if (!S->mg[k]) continue;
-        // two guess kernels; the start check and the zeroing kernel (mixed
-        // precision: norm, zeroing and the refinement residual)
-        const int start = S->prm.mg_precision == VDI_MG_MIXED ? 3 : 2;
-        launches += out->solves[k] * (2 + start) +
+        // the guess kernel; the start check (mixed precision: norm, zeroing
+        // and the refinement residual)
+        const int start = S->prm.mg_precision == VDI_MG_MIXED ? 3 : 1;
+        launches += out->solves[k] * (1 + start) +
                     out->vcycles[k] * mg_kernels_per_iteration(S->mg[k], S->prm.mg_precision);
     }
     out->kernel_launches = launches;

@@ -634,85 +634,71 @@ __global__ void k_vel_update(Grid g, Fields f, CellView c0v, CellView c1v, const
 
 // ------------------------------------------------ multigrid initial guess
 // mgs_common::initial_guess (mgs_common.cc:17-50). The decision is made from
-// device-resident times so that a captured graph replays it correctly.
-__global__ void k_guess_apply(double* __restrict__ z, double* __restrict__ zprev, int n, const GuessHist* h,
-                              const double* d_time) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    int sc = h->scount;
-    if (sc < 2) {
-        if (sc == 1) zprev[k] = z[k];
-        return;
+// device-resident times so that a captured graph replays it correctly. One
+// launch: thread 0 of every block copies the history to shared memory, and
+// the last block to arrive (an atomic count in the history itself) advances
+// the history, after every block has read the old one.
+//
+// QUAD adds a second-order variant: with three past solutions z (at t0),
+// zprev (t_prev) and zprev2 (t_prev2) the guess is the quadratic Lagrange
+// extrapolation to t; with two it is the linear rule. This changes only the
+// starting iterate of the solve, not its converged result.
+//
+// The target time is *d_time + tadd: a guess enqueued before the kernel that
+// advances the clock by dt/2 passes tadd = dt/2 and gets the same double that
+// the clock will hold (the same single rounded addition).
+template <bool QUAD>
+__global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, double* __restrict__ zprev2, int n,
+                        GuessHist* h, const double* d_time, double tadd, int* err) {
+    __shared__ double s_t[4];   // t, t0, t_prev, t_prev2
+    __shared__ int s_sc;
+    if (threadIdx.x == 0) {
+        s_t[0] = *d_time + tadd;
+        s_t[1] = h->t0;
+        s_t[2] = h->t_prev;
+        s_t[3] = h->t_prev2;
+        s_sc = h->scount;
     }
-    double t = *d_time;
-    if (fabs(h->t0 - h->t_prev) < 2.220446049250313e-16 * 10) return;
-    double a = 1. / (h->t0 - h->t_prev), b = (t - h->t_prev) * a, cc = (t - h->t0) * a;
-    double zz = z[k];
-    z[k] = b * zz - cc * zprev[k];
-    zprev[k] = zz;
-}
-
-__global__ void k_guess_finish(GuessHist* h, const double* d_time, int* err) {
-    double t = *d_time;
-    if (h->scount < 2) {
-        if (h->scount == 1) h->t0 = t;
-        else h->t_prev = t;
-        h->scount++;
-    } else {
-        if (fabs(h->t0 - h->t_prev) < 2.220446049250313e-16 * 10) {
-            atomicOr(err, DEV_DUP_TIME);
-            return;
+    __syncthreads();
+    const int sc = s_sc;
+    const double t = s_t[0], t0 = s_t[1], t1 = s_t[2];
+    const bool dup = fabs(t0 - t1) < 2.220446049250313e-16 * 10;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        if (sc < 2) {
+            if (sc == 1) zprev[k] = z[k];
+        } else if (!dup) {
+            double zz = z[k];
+            if (!QUAD || sc == 2) {
+                double a = 1. / (t0 - t1), b = (t - t1) * a, cc = (t - t0) * a;
+                z[k] = b * zz - cc * zprev[k];
+            } else {
+                double t2 = s_t[3];
+                double l0 = (t - t1) * (t - t2) / ((t0 - t1) * (t0 - t2));
+                double l1 = (t - t0) * (t - t2) / ((t1 - t0) * (t1 - t2));
+                double l2 = (t - t0) * (t - t1) / ((t2 - t0) * (t2 - t1));
+                z[k] = l0 * zz + l1 * zprev[k] + l2 * zprev2[k];
+            }
+            if (QUAD) zprev2[k] = zprev[k];
+            zprev[k] = zz;
         }
-        h->t_prev = h->t0;
-        h->t0 = t;
     }
-}
-
-/** Second-order variant of k_guess_apply: with three past solutions z (at
- * t0), zprev (t_prev) and zprev2 (t_prev2) the guess is the quadratic
- * Lagrange extrapolation to t; with two it is the linear rule above. This
- * changes only the starting iterate of the solve, not its converged result. */
-__global__ void k_guess2_apply(double* __restrict__ z, double* __restrict__ zprev, double* __restrict__ zprev2, int n,
-                               const GuessHist* h, const double* d_time) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    int sc = h->scount;
+    if (threadIdx.x != 0) return;
+    __threadfence();
+    if (atomicAdd(&h->arrive, 1u) != gridDim.x - 1) return;
+    __threadfence();
+    h->arrive = 0;
     if (sc < 2) {
-        if (sc == 1) zprev[k] = z[k];
-        return;
-    }
-    double t = *d_time, t0 = h->t0, t1 = h->t_prev;
-    if (fabs(t0 - t1) < 2.220446049250313e-16 * 10) return;
-    double zz = z[k];
-    if (sc == 2) {
-        double a = 1. / (t0 - t1), b = (t - t1) * a, cc = (t - t0) * a;
-        z[k] = b * zz - cc * zprev[k];
-    } else {
-        double t2 = h->t_prev2;
-        double l0 = (t - t1) * (t - t2) / ((t0 - t1) * (t0 - t2));
-        double l1 = (t - t0) * (t - t2) / ((t1 - t0) * (t1 - t2));
-        double l2 = (t - t0) * (t - t1) / ((t2 - t0) * (t2 - t1));
-        z[k] = l0 * zz + l1 * zprev[k] + l2 * zprev2[k];
-    }
-    zprev2[k] = zprev[k];
-    zprev[k] = zz;
-}
-
-__global__ void k_guess2_finish(GuessHist* h, const double* d_time, int* err) {
-    double t = *d_time;
-    if (h->scount < 2) {
-        if (h->scount == 1) h->t0 = t;
+        if (sc == 1) h->t0 = t;
         else h->t_prev = t;
-        h->scount++;
+        h->scount = sc + 1;
+    } else if (dup) {
+        atomicOr(err, DEV_DUP_TIME);
     } else {
-        if (fabs(h->t0 - h->t_prev) < 2.220446049250313e-16 * 10) {
-            atomicOr(err, DEV_DUP_TIME);
-            return;
-        }
-        h->t_prev2 = h->t_prev;
-        h->t_prev = h->t0;
+        if (QUAD) h->t_prev2 = t1;
+        h->t_prev = t0;
         h->t0 = t;
-        if (h->scount < 3) h->scount++;
+        if (QUAD && sc < 3) h->scount = sc + 1;
     }
 }
 
@@ -785,16 +771,13 @@ int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c
     k_vel_update<<<cell_grid(g, 1), cell_block(g), 0, s>>>(g, f, c0, c1, z, dt);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
-int launch_guess2(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,
-                  const double* d_time, int* err) {
-    k_guess2_apply<<<(n + 255) / 256, 256, 0, s>>>(z, zprev, zprev2, n, h, d_time);
-    k_guess2_finish<<<1, 1, 0, s>>>(h, d_time, err);
-    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
-}
-
-int launch_guess(cudaStream_t s, double* z, double* zprev, int n, GuessHist* h, const double* d_time, int* err) {
-    k_guess_apply<<<(n + 255) / 256, 256, 0, s>>>(z, zprev, n, h, d_time);
-    k_guess_finish<<<1, 1, 0, s>>>(h, d_time, err);
+int launch_guess(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,
+                 const double* d_time, double tadd, int quadratic, int* err) {
+    if (n <= 0) return VDI_OK;
+    if (quadratic)
+        k_guess<true><<<(n + 255) / 256, 256, 0, s>>>(z, zprev, zprev2, n, h, d_time, tadd, err);
+    else
+        k_guess<false><<<(n + 255) / 256, 256, 0, s>>>(z, zprev, zprev2, n, h, d_time, tadd, err);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 

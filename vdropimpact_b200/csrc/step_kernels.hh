@@ -51,6 +51,7 @@ struct GasStats {
 /** Time-extrapolation history of one solver (mgs_common.hh:21-36). */
 struct GuessHist {
     int scount;
+    unsigned arrive;    // blocks of the current guess launch that have read the history
     double t_prev, t0;
     double t_prev2;     // time of the third-latest solution (quadratic guess)
 };
@@ -80,11 +81,12 @@ int launch_fem_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs
                    double a_cc_edge, double a_cc_mid, double* src);
 int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c0, CellView c1, const double* z,
                       double dt);
-int launch_guess(cudaStream_t s, double* z, double* zprev, int n, GuessHist* h, const double* d_time, int* err);
-/** Quadratic-in-time extrapolation from the last three solutions (zprev2 the
- * oldest); falls back to the reference's linear rule until three exist. */
-int launch_guess2(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,
-                  const double* d_time, int* err);
+/** One launch of the initial guess at time *d_time + tadd: the reference's
+ * linear rule, or (quadratic != 0) quadratic-in-time extrapolation from the
+ * last three solutions (zprev2 the oldest, unused by the linear rule), which
+ * falls back to the linear rule until three exist. */
+int launch_guess(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,
+                 const double* d_time, double tadd, int quadratic, int* err);
 
 /** Gas-layer update (gas_layer::update, gas_layer.cc:36-46) as one CTA.
  * Also advances *d_time by dt/2 (fluid_2d.cc:102). */
