@@ -285,10 +285,16 @@ int vdi_mg_apply(vdi_mg* mg, const double* d_z, double* d_y);
  * events on the system's stream, which = 0 the finest-level
  * pre-smoothing/restriction kernel, 1 the finest prolongation/post-smoothing
  * kernel, 2 a whole FP64 V-cycle (the ms per V-cycle that mg_test.cc:36-43
- * reports), 3 the single-CTA coarse cycle alone; returns the mean duration
- * and the algorithmic bytes per launch (0 for which = 3). */
+ * reports), 3 the single-launch coarse cycle alone; returns the mean
+ * duration and the algorithmic bytes per launch (0 for which = 3). */
 int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
                    double* bytes_per_launch);
+/* The coarse levels of a V-cycle (of the given vdi_mg_precision) that run in
+ * one launch: the first such level (level 0 the finest; -1 when the
+ * hierarchy has none) and the CTAs of that launch (1: a single CTA; 8 or
+ * 16: a thread-block cluster whose CTAs hold row slabs of every level). No
+ * reference counterpart. */
+int vdi_mg_coarse_cycle(const vdi_mg* mg, int precision, int* first_level, int* ctas);
 
 /* ------------------------------------------------------------ U-Net
  * The learned initial guess has no counterpart in the reference. A small

@@ -408,6 +408,15 @@ class _MgSystem:
                                    C.c_void_p(self.z.data_ptr()), C.byref(ms), C.byref(by)), "vdi_mg_profile")
         return ms.value, by.value
 
+    def coarse_cycle(self, precision=None):
+        """(first level, CTAs) of the single-launch coarse cycle of a V-cycle
+        in this precision: CTAs 1 for one CTA, 8 or 16 for a cluster; first
+        level -1 when the hierarchy has none."""
+        first, ctas = C.c_int(), C.c_int()
+        check(lib().vdi_mg_coarse_cycle(self._h, _PREC[precision or self.precision], C.byref(first),
+                                        C.byref(ctas)), "vdi_mg_coarse_cycle")
+        return first.value, ctas.value
+
     def residual(self):
         """(r, ||r||_2) with r = b - A z (tgmg::output_res)."""
         torch = _torch()

@@ -142,6 +142,7 @@ _SIGS = [
     ("vdi_mg_apply", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("vdi_mg_profile", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_float),
                                  _dp]),
+    ("vdi_mg_coarse_cycle", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("vdi_unet_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint, C.c_void_p, C.POINTER(C.c_void_p)]),
     ("vdi_unet_destroy", C.c_int, [C.c_void_p]),
     ("vdi_unet_param_count", C.c_long, [C.c_void_p]),

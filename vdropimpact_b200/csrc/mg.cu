@@ -26,6 +26,8 @@
 // inside FP64 iterative refinement use the same kernels with T = float.
 #include "vdi_internal.hh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstdlib>
 #include <cmath>
@@ -229,24 +231,40 @@ __device__ __forceinline__ T op_relaxed(const OP& c, const T* w, T bv, int P, in
 }
 
 /** Bilinear cell-centred prolongation of the coarse correction to fine cell
- * (i,j); ghost values are g * (boundary value) on each side. */
-template <typename T, typename TC>
-__device__ __forceinline__ T cc_interp(const CCc<T>& f, const TC* zc, int i, int j) {
-    const int mc = f.m >> 1, nc = f.n >> 1;
-    int I = i >> 1, J = j >> 1;
-    int sx = (i & 1) ? 1 : -1, sy = (j & 1) ? 1 : -1;
-    int Ix = I + sx, Jy = J + sy;
-    bool xo = Ix < 0 || Ix >= mc, yo = Jy < 0 || Jy >= nc;
-    T gx = T(sx < 0 ? f.gL : f.gR), gy = T(sy < 0 ? f.gD : f.gU);
-    T c00 = T(zc[I + mc * J]);
-    T c10 = xo ? gx * c00 : T(zc[Ix + mc * J]);
-    T c01 = yo ? gy * c00 : T(zc[I + mc * Jy]);
+ * (i,j) from coarse row r0 = J = j/2 and its neighbour row r1 = J +- 1 (yo:
+ * that row is outside the grid, gy its ghost factor); ghost values are
+ * g * (boundary value) on each side. */
+template <typename T, typename RT>
+__device__ __forceinline__ T cc_interp_r(const CCc<T>& f, const RT* r0, const RT* r1, bool yo, T gy, int i) {
+    const int mc = f.m >> 1;
+    int I = i >> 1;
+    int sx = (i & 1) ? 1 : -1;
+    int Ix = I + sx;
+    bool xo = Ix < 0 || Ix >= mc;
+    T gx = T(sx < 0 ? f.gL : f.gR);
+    T c00 = T(r0[I]);
+    T c10 = xo ? gx * c00 : T(r0[Ix]);
+    T c01 = yo ? gy * c00 : T(r1[I]);
     T c11;
     if (xo && yo) c11 = gx * gy * c00;
     else if (xo) c11 = gx * c01;
     else if (yo) c11 = gy * c10;
-    else c11 = T(zc[Ix + mc * Jy]);
+    else c11 = T(r1[Ix]);
     return T(0.5625) * c00 + T(0.1875) * (c10 + c01) + T(0.0625) * c11;
+}
+/** The same with row(J) giving coarse row J (indexable by coarse column). */
+template <typename T, class ROW>
+__device__ __forceinline__ T cc_interp_rows(const CCc<T>& f, ROW row, int i, int j) {
+    const int nc = f.n >> 1;
+    const int J = j >> 1, sy = (j & 1) ? 1 : -1, Jy = J + sy;
+    const bool yo = Jy < 0 || Jy >= nc;
+    const T gy = T(sy < 0 ? f.gD : f.gU);
+    return cc_interp_r(f, row(J), yo ? row(J) : row(Jy), yo, gy, i);
+}
+template <typename T, typename TC>
+__device__ __forceinline__ T cc_interp(const CCc<T>& f, const TC* zc, int i, int j) {
+    const int mc = f.m >> 1;
+    return cc_interp_rows(f, [&](int J) { return zc + mc * J; }, i, j);
 }
 
 /** Bilinear prolongation of node-centred corrections to fine node (i,j). */
@@ -1038,6 +1056,7 @@ __global__ void sub_mean_k(const double* src, double* dst, long N, const double*
 }
 
 #include "mg_general.cuh"
+#include "mg_cluster.cuh"
 
 class MG {
   public:
@@ -1069,6 +1088,14 @@ class MG {
     int dlev = -1;
     double* dinv64 = nullptr;
     float* dinv32 = nullptr;
+    // the cluster-resident coarse cycle (mg_cluster.cuh) of the FP64 and FP32
+    // V-cycles: its top level (-1: not used), CTAs and shared memory per CTA
+    struct ClusterPlan {
+        int top = -1, cs = 0;
+        size_t smem = 0;
+    };
+    ClusterPlan cl64, cl32;
+    bool allow_cluster = true;   // false where the exact coarsest level cannot be set up
     int nu1 = 2, nu2 = 2;
     double rtol = 1e-10;
     int max_it = 200;
@@ -1201,12 +1228,14 @@ class MG {
         nmulti64 = nmulti32 = 0;
         smooth_tail = false;
         smem64 = smem32 = 0;
+        cl64 = cl32 = ClusterPlan{};
         general = true;
         return VDI_OK;
     }
 
     int build_fast_levels() {
         lv.clear();
+        cl64 = cl32 = ClusterPlan{};
         if (fem()) {
             double dydx = c2 / c1, dxdy = c1 / c2;
             // mgs_fem.cc:8-11
@@ -1273,8 +1302,83 @@ class MG {
         }
         smem64 = tail_bytes(nmulti64, 8);
         smem32 = tail_bytes(nmulti32, 4);
+        cl64 = plan_cluster<double>();
+        cl32 = plan_cluster<float>();
+        if (cl64.top >= 0) nmulti64 = cl64.top;
+        if (cl32.top >= 0) nmulti32 = cl32.top;
         return VDI_OK;
     }
+
+    /** Shared-memory layout of the cluster cycle from level `top` (cs CTAs):
+     * fills a when given; returns the elements per CTA. */
+    template <typename T>
+    long cluster_layout(int top, int cs, int dl, CCClusterArgs<T>* a) const {
+        long off = 0;
+        for (int q = 0; top + q < dl; q++) {
+            const int l = top + q;
+            const long mm = lv[l].m, h = lv[l].n / cs;
+            if (a) {
+                a->lv[q] = ccc<T>(l);
+                a->h[q] = int(h);
+                a->oz[q] = int(off);
+                a->ob[q] = int(off + (h + 2 * CL_G) * mm);
+                a->opre[q] = int(off + 2 * (h + 2 * CL_G) * mm);
+                a->opost[q] = int(off + 2 * (h + 2 * CL_G) * mm + 8 * mm);
+            }
+            off += 2 * (h + 2 * CL_G) * mm + 8 * mm + (q > 0 ? 6 * mm : 0);
+        }
+        if (a) {
+            a->nd = dl - top;
+            a->cs = cs;
+            a->dl = ccc<T>(dl);
+            a->ostage = int(off);
+        }
+        off += size(dl - 1);
+        if (a) a->odb = int(off);
+        off += size(dl);
+        if (a) a->odz = int(off);
+        off += size(dl);
+        return off;
+    }
+
+    /** The cluster cycle for this hierarchy, if it applies: cell-centred
+     * systems with an exact coarsest level whose finer neighbour splits into
+     * equal row slabs; the top level is the finest whose slabs fit in shared
+     * memory. VDI_MG_CLUSTER=0 turns it off. */
+    template <typename T>
+    ClusterPlan plan_cluster() const {
+        ClusterPlan p;
+        const char* e = getenv("VDI_MG_CLUSTER");
+        if ((e && atoi(e) == 0) || !allow_cluster || fem() || smooth_tail || neumann() || general) return p;
+        int dl = -1;
+        for (int l = 0; l < nlev; l++)
+            if (size(l) <= DIRECT_MAX) {
+                dl = l;
+                break;
+            }
+        if (dl < 1) return p;
+        if (cc_cluster_attr<T>() != cudaSuccess) {
+            cudaGetLastError();
+            return p;
+        }
+        for (int cs : {16, 8}) {
+            if (lv[dl - 1].n % cs) continue;
+            for (int top = std::max(0, dl - CL_MAXLEV); top < dl; top++) {
+                // a thread owns one column of the widest slab level
+                if (lv[top].m > CL_THREADS) continue;
+                const size_t bytes = size_t(cluster_layout<T>(top, cs, dl, nullptr)) * sizeof(T);
+                if (bytes > CL_SMEM_LIMIT) continue;
+                if (cc_cluster_fits<T>(cs, bytes) <= 0) break;
+                p.top = top;
+                p.cs = cs;
+                p.smem = bytes;
+                return p;
+            }
+        }
+        return p;
+    }
+    const ClusterPlan& cplan(double*) const { return cl64; }
+    const ClusterPlan& cplan(float*) const { return cl32; }
 
     int alloc() {
         if (neumann()) {
@@ -1360,8 +1464,7 @@ class MG {
      * DIRECT_MAX unknowns, its operator probed into a stencil and inverted. */
     int setup_direct() {
         if (smooth_tail || general || neumann()) return VDI_OK;
-        int from = std::max(nmulti64, nmulti32);
-        for (int l = std::max(from, 0); l < nlev; l++)
+        for (int l = 0; l < nlev; l++)
             if (size(l) <= DIRECT_MAX) {
                 dlev = l;
                 break;
@@ -1409,6 +1512,17 @@ class MG {
             launch_cc_tile<T, 0>(s, ccc<T>(l), a);
             VDI_CUDA(cudaGetLastError());
             return VDI_OK;
+        }
+        if (l == nmulti && cplan(static_cast<T*>(nullptr)).top == l) {
+            const ClusterPlan& cp = cplan(static_cast<T*>(nullptr));
+            if (dlev < 0 || !dinv(static_cast<T*>(nullptr))) {
+                set_error("multigrid: the cluster cycle needs the exact coarsest level");
+                return VDI_ERR_CUDA;
+            }
+            CCClusterArgs<T> a{};
+            cluster_layout<T>(l, cp.cs, dlev, &a);
+            a.dinv = dinv(static_cast<T*>(nullptr));
+            return launch_cc_cluster<T>(s, a, cp.smem, b, z, zero_init);
         }
         if (l == nmulti) {
             if (fem()) {
@@ -1654,6 +1768,18 @@ int mg_set_cta_limit(MG* mg, size_t bytes) {
 }
 
 size_t mg_cta_limit(const MG* mg) { return mg->cta_limit; }
+int mg_coarse_cycle(const MG* mg, int precision, int* first, int* ctas) {
+    const bool f32 = precision == VDI_MG_MIXED;
+    if (mg->general || mg->smooth_tail) {
+        *first = -1;
+        *ctas = 0;
+        return VDI_OK;
+    }
+    const auto& cp = f32 ? mg->cl32 : mg->cl64;
+    *first = f32 ? mg->nmulti32 : mg->nmulti64;
+    *ctas = cp.top >= 0 ? cp.cs : 1;
+    return VDI_OK;
+}
 int mg_tiled_levels(const MG* mg, int precision) {
     if (mg->general) return -1;
     return precision == VDI_MG_MIXED ? mg->nmulti32 : mg->nmulti64;
@@ -1936,6 +2062,7 @@ int noalloc_base(int dev, unsigned char** out) {
 int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
     MG* g = new MG();
     g->kind = k.kind; g->m = k.m; g->n = k.n; g->c1 = k.c1; g->c2 = k.c2; g->x_sym = k.x_sym;
+    g->allow_cluster = false;   // its inverse would need an allocation
     int st = g->build_levels();
     if (st == VDI_OK && g->general) {
         set_error("vdi_mg_solve_noalloc: a %dx%d grid needs the general hierarchy, which allocates", k.m, k.n);

@@ -896,6 +896,11 @@ int vdi_mg_apply(vdi_mg* h, const double* d_z, double* d_y) {
     return VDI_OK;
 }
 
+int vdi_mg_coarse_cycle(const vdi_mg* h, int precision, int* first_level, int* ctas) {
+    if (!h || !first_level || !ctas) return VDI_ERR_INVALID_ARGUMENT;
+    return mg_coarse_cycle(h->g, precision, first_level, ctas);
+}
+
 int vdi_mg_profile(vdi_mg* h, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
                    double* bytes_per_launch) {
     if (!h || !d_b || !d_z || !ms_per_launch || !bytes_per_launch || which < 0 || which > 3)

@@ -96,6 +96,9 @@ void mg_destroy(MG* mg);
 /** Bytes below which levels run in the single-CTA cycle (rebuilds). */
 int mg_set_cta_limit(MG* mg, size_t bytes);
 size_t mg_cta_limit(const MG* mg);
+/** First level of the single-launch coarse cycle (-1: none) and the CTAs it
+ * runs on (1: one CTA; more: a cluster). */
+int mg_coarse_cycle(const MG* mg, int precision, int* first, int* ctas);
 /** Tiled (per-launch) levels of the hierarchy for a precision; -1 for the
  * general hierarchy. */
 int mg_tiled_levels(const MG* mg, int precision);
