@@ -869,18 +869,37 @@ __device__ __forceinline__ void grid_ij(const OP& c, long k, int& i, int& j) {
     i = int(k - long(j) * op_m(c));
 }
 
+/** Grid-stride walk over the m-wide grid's points 0 <= k < tot: calls
+ * f(k, i, j) with (i, j) advanced incrementally (two divisions per thread,
+ * none per point). */
+template <class F>
+__device__ __forceinline__ void grid_walk(int m, long tot, F f) {
+    const long stride = long(gridDim.x) * blockDim.x;
+    long k = blockIdx.x * long(blockDim.x) + threadIdx.x;
+    if (k >= tot) return;
+    int j = int(k / m), i = int(k - long(j) * m);
+    const int sj = int(stride / m), si = int(stride - long(sj) * m);
+    for (; k < tot; k += stride) {
+        f(k, i, j);
+        i += si;
+        j += sj;
+        if (i >= m) {
+            i -= m;
+            j++;
+        }
+    }
+}
+
 /** ||b - A z||^2 accumulated in FP64, then the solve decision. */
 template <typename T, class OP>
 __global__ void resid_norm_k(OP c, const T* __restrict__ z, const T* __restrict__ b, Reduce rd, SolveCtl* ctl,
                              int count_cycle, int use_cond, cudaGraphConditionalHandle h) {
     double s = 0;
     const long tot = long(op_m(c)) * op_n(c);
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
-        int i, j;
-        grid_ij(c, k, i, j);
+    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
         double r = double(op_resid(c, z + k, b[k], op_m(c), i, j));
         s += r * r;
-    }
+    });
     s = block_sum(s);
     double total;
     if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
@@ -896,14 +915,12 @@ __global__ void first_check_k(OP c, T* __restrict__ z, const T* __restrict__ b, 
     __shared__ int zero_src;
     double sb = 0, sr = 0;
     const long tot = long(op_m(c)) * op_n(c);
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
-        int i, j;
-        grid_ij(c, k, i, j);
+    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
         double bv = double(b[k]);
         double r = double(op_resid(c, z + k, b[k], op_m(c), i, j));
         sb += bv * bv;
         sr += r * r;
-    }
+    });
     sb = block_sum(sb);
     __syncthreads();
     sr = block_sum(sr);
@@ -930,13 +947,11 @@ __global__ void resid_to32_k(OP c, const double* __restrict__ z, const double* _
                              cudaGraphConditionalHandle h) {
     double s = 0;
     const long tot = long(op_m(c)) * op_n(c);
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
-        int i, j;
-        grid_ij(c, k, i, j);
+    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
         double r = op_resid(c, z + k, b[k], op_m(c), i, j);
         r32[k] = float(r);
         s += r * r;
-    }
+    });
     s = block_sum(s);
     double total;
     if (grid_sum(s, rd, &total) && threadIdx.x == 0) solve_decide(ctl, total, count_cycle, use_cond, h);
@@ -957,13 +972,11 @@ __global__ void resid_out_k(OP c, const T* __restrict__ z, const T* __restrict__
                             double* out) {
     double s = 0;
     const long tot = long(op_m(c)) * op_n(c);
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
-        int i, j;
-        grid_ij(c, k, i, j);
+    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
         T v = op_resid(c, z + k, b[k], op_m(c), i, j);
         if (r) r[k] = v;
         s += double(v) * double(v);
-    }
+    });
     s = block_sum(s);
     double total;
     if (grid_sum(s, rd, &total) && threadIdx.x == 0) *out = sqrt(total);
@@ -997,7 +1010,17 @@ __global__ void add_f32_to_f64(double* __restrict__ z, const float* __restrict__
 
 // =================================================================== host
 static inline int nblk(long n, int t = 256) { return int((n + t - 1) / t); }
-static inline int rblocks(long n) { return std::max(1, std::min(MAX_PARTIALS, nblk(n, 256))); }
+/** Blocks of 256 threads that the current GPU holds at once: 6 per SM for
+ * the reduction kernels' 40 registers per thread. */
+static inline int resident_blocks() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+    return 6 * std::max(1, sms);
+}
+/** Blocks of a whole-grid reduction over n points: one resident wave at
+ * most, so the partial sums stay few and the last block's sum short. */
+static inline int rblocks(long n) { return std::max(1, std::min({MAX_PARTIALS, nblk(n, 256), resident_blocks()})); }
 
 /** Per-level description in double precision, converted per precision. */
 struct LevelD {
@@ -1691,7 +1714,7 @@ class MG {
             VDI_CUDA(cudaGetLastError());
             return enqueue_resid32(s, b, z, 0, use_cond, h);
         }
-        int nb = std::max(1, std::min(MAX_PARTIALS / 2, nblk(N, 256)));
+        int nb = std::max(1, std::min({MAX_PARTIALS / 2, nblk(N, 256), resident_blocks()}));
         if (general)
             first_check_k<double><<<nb, 256, 0, s>>>(gen.op(0), z, b, rd, ctl, use_cond, h);
         else if (fem())

@@ -651,36 +651,41 @@ template <bool QUAD>
 __global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, double* __restrict__ zprev2, int n,
                         GuessHist* h, const double* d_time, double tadd, int* err) {
     __shared__ double s_t[4];   // t, t0, t_prev, t_prev2
-    __shared__ int s_sc;
+    __shared__ int s_sc, s_head;
     if (threadIdx.x == 0) {
         s_t[0] = *d_time + tadd;
         s_t[1] = h->t0;
         s_t[2] = h->t_prev;
         s_t[3] = h->t_prev2;
         s_sc = h->scount;
+        s_head = h->head;
     }
     __syncthreads();
     const int sc = s_sc;
     const double t = s_t[0], t0 = s_t[1], t1 = s_t[2];
     const bool dup = fabs(t0 - t1) < 2.220446049250313e-16 * 10;
+    // quadratic history: h1 holds the solution at t_prev, h2 the one at
+    // t_prev2; the newest history replaces h2's and the two swap roles
+    double* h1 = (QUAD && s_head) ? zprev2 : zprev;
+    double* h2 = (QUAD && s_head) ? zprev : zprev2;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
         if (sc < 2) {
-            if (sc == 1) zprev[k] = z[k];
+            if (sc == 1) h1[k] = z[k];
         } else if (!dup) {
             double zz = z[k];
             if (!QUAD || sc == 2) {
                 double a = 1. / (t0 - t1), b = (t - t1) * a, cc = (t - t0) * a;
-                z[k] = b * zz - cc * zprev[k];
+                z[k] = b * zz - cc * h1[k];
             } else {
                 double t2 = s_t[3];
                 double l0 = (t - t1) * (t - t2) / ((t0 - t1) * (t0 - t2));
                 double l1 = (t - t0) * (t - t2) / ((t1 - t0) * (t1 - t2));
                 double l2 = (t - t0) * (t - t1) / ((t2 - t0) * (t2 - t1));
-                z[k] = l0 * zz + l1 * zprev[k] + l2 * zprev2[k];
+                z[k] = l0 * zz + l1 * h1[k] + l2 * h2[k];
             }
-            if (QUAD) zprev2[k] = zprev[k];
-            zprev[k] = zz;
+            if (QUAD) h2[k] = zz;
+            else h1[k] = zz;
         }
     }
     if (threadIdx.x != 0) return;
@@ -695,7 +700,10 @@ __global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, doub
     } else if (dup) {
         atomicOr(err, DEV_DUP_TIME);
     } else {
-        if (QUAD) h->t_prev2 = t1;
+        if (QUAD) {
+            h->t_prev2 = t1;
+            h->head = s_head ^ 1;
+        }
         h->t_prev = t0;
         h->t0 = t;
         if (QUAD && sc < 3) h->scount = sc + 1;

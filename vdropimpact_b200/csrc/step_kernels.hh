@@ -54,6 +54,7 @@ struct GuessHist {
     unsigned arrive;    // blocks of the current guess launch that have read the history
     double t_prev, t0;
     double t_prev2;     // time of the third-latest solution (quadratic guess)
+    int head;           // quadratic guess: 1 when zprev2 holds the t_prev solution
 };
 
 /** A read-only view of a cell array with an arbitrary pitch and origin. */
