@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define VDI_ABI_VERSION 1
+#define VDI_ABI_VERSION 2
 
 /* ---------------------------------------------------------------- status */
 enum vdi_status {
@@ -70,6 +70,12 @@ typedef struct vdi_params {
     int mg_max_vcycles;       /* V-cycle cap per solve (default 200) */
     int mg_precision;         /* VDI_MG_FP64 or VDI_MG_MIXED */
     int mg_guess;             /* VDI_GUESS_EXTRAPOLATE or VDI_GUESS_LEARNED */
+    /* tracers and the non-inertial frame (fileinfo.cc:59, 96-101, 179-191) */
+    int ntrace;               /* tracers advected with the flow (0: none) */
+    int nif_mode;             /* 0 off; 1 frame velocity at the centre
+                                 (nif_center); 2 averaged over columns
+                                 [nif_a, nif_b) (nif_range) */
+    int nif_a, nif_b;         /* the nif_range window (fileinfo.cc:182-187) */
 } vdi_params;
 
 enum vdi_mg_precision {
@@ -91,8 +97,8 @@ int vdi_params_from_cfg(const char* cfg_text, vdi_params* out);
 
 /* Run and output options of a .cfg text (fileinfo.cc:56-122): the output
  * flags (fflags bits of the 'output' keyword), restart frequency, tracer count
- * and machine-readable timing flag. Keywords outside the GPU path
- * (gas_layer_data, nif_center, nif_range) return VDI_ERR_CONFIG. */
+ * and machine-readable timing flag. The data-driven gas layer
+ * (gas_layer_data) is outside the GPU path and returns VDI_ERR_CONFIG. */
 typedef struct vdi_run_options {
     unsigned int fflags;      /* 1 u, 2 v, 4 p, 8 pb, 16 pbfull, 32 w, 64 h, 128 fbd,
                                  256 pg, 512 hfull, 1024 fbdfull, 2048 pgfull */
@@ -138,6 +144,14 @@ typedef struct vdi_state {
 } vdi_state;
 int vdi_sim_get_state(vdi_sim* sim, vdi_state* h_state);
 int vdi_sim_set_state(vdi_sim* sim, const vdi_state* h_state);
+/* The tracer positions x0, y0, x1, y1, ... (count = 2 * ntrace doubles; the
+ * reference's tm array, fluid_2d.hh:49-50). vdi_sim_init_fields places them
+ * with the C library's rand() as fluid_2d::init_tracers does
+ * (fluid_2d.cc:495-502), so a process that has not called rand() before
+ * gets the reference's positions; each step moves them first
+ * (fluid_2d::update_tracers, fluid_2d.cc:507-526). */
+int vdi_sim_get_tracers(vdi_sim* sim, double* h_xy, long count);
+int vdi_sim_set_tracers(vdi_sim* sim, const double* h_xy, long count);
 
 /* Per-solver statistics since the last reset (the reference's
  * tgmg_predict::avg_iters and wall-clock counters, mgs_common.hh:47-55). */

@@ -25,6 +25,12 @@
 //                                       gas-layer height h[m], the per-step
 //                                       input of the lift-off analysis
 //                                       (tt_analysis.cc:97-164)
+//   tracers <cfg> <nsteps> <out>        from init_fields (tracers placed with
+//                                       rand(), fluid_2d.cc:495-502), nsteps
+//                                       steps; writes for steps 0..nsteps the
+//                                       time, Vframe and the 2*ntrace tracer
+//                                       coordinates (fluid_2d.cc:507-526,
+//                                       fluid_2d_sio.cc:228-253)
 //   tri  <n> <abcd> <out> [thomas]      tri_solve::solve_lapack
 //                                       (tri_solve.cc:24-33) or solve()
 //                                       (tri_solve.cc:37-49)
@@ -178,6 +184,28 @@ static int run_heights(char** argv) {
     return 0;
 }
 
+static void tracer_row(fluid_2d& f,std::vector<double>& rows) {
+    rows.push_back(f.time);
+    rows.push_back(gls(f)->Vframe);
+    rows.insert(rows.end(),f.tm,f.tm+2*f.ntrace);
+}
+
+static int run_tracers(char** argv) {
+    fluid_2d f(argv[2]);
+    int nsteps=atoi(argv[3]);
+    f.init_fields();
+    double dt=frame_dt(f);
+    std::vector<double> rows;
+    tracer_row(f,rows);
+    for(int k=1;k<=nsteps;k++) {
+        f.step_forward(dt);
+        tracer_row(f,rows);
+    }
+    write_doubles(argv[4],&rows[0],rows.size());
+    printf("{\"steps\": %d, \"dt\": %.17g, \"ntrace\": %d}\n",nsteps,dt,f.ntrace);
+    return 0;
+}
+
 template<class T>
 static int solve_one(T& msu,const char* zfile) {
     msu.mg.setup();
@@ -195,6 +223,7 @@ int main(int argc,char** argv) {
     if(strcmp(cmd,"dump")==0&&argc>=6) return run_steps(argc,argv,true,false);
     if(strcmp(cmd,"time")==0&&argc>=4) return run_steps(argc,argv,false,true);
     if(strcmp(cmd,"heights")==0&&argc>=5) return run_heights(argv);
+    if(strcmp(cmd,"tracers")==0&&argc>=5) return run_tracers(argv);
     if((strcmp(cmd,"mac")==0||strcmp(cmd,"fem")==0)&&argc>=8) {
         int m=atoi(argv[2]),n=atoi(argv[3]);
         double dx=atof(argv[4]),dy=atof(argv[5]);

@@ -59,6 +59,10 @@ class Params:
     Pamb: float
     x_sym: bool = False
     implicit_visc: bool = False
+    # tracers and the non-inertial frame (fileinfo.cc:59, 96-101)
+    ntrace: int = 0
+    nif_mode: int = 0
+    nif_r: float = 0.
     # derived
     mu: float = field(init=False)
     muinv: float = field(init=False)
@@ -77,6 +81,8 @@ class Params:
     xxsp: float = field(init=False)
     yysp: float = field(init=False)
     dt_reg: float = field(init=False)
+    nif_a: int = field(init=False)
+    nif_b: int = field(init=False)
 
     def __post_init__(self):
         # fileinfo.cc:142-152
@@ -108,6 +114,19 @@ class Params:
             self.dt_reg = self.dx * self.tmult
         else:
             self.dt_reg = self.dx * self.dx * self.rho * self.muinv * self.tmult * 0.25
+        # fileinfo.cc:179-191: the nif_range window of columns
+        self.nif_a = self.nif_b = 0
+        if self.nif_mode == 2:
+            b = int((self.nif_r - self.ax) * self.xsp + 0.5)
+            if b >= self.m:
+                b = self.m - 1
+            if self.x_sym:
+                a = 0
+            else:
+                a = max(0, int((-self.nif_r - self.ax) * self.xsp + 0.5))
+            if b - a <= 0:
+                raise OracleError("Velocity window for non-inertial frame is too small")
+            self.nif_a, self.nif_b = a, b
 
     def timestep_select(self, interval: float):
         """fluid_2d.hh:82-86: largest dt <= dt_reg that divides interval."""
@@ -148,9 +167,14 @@ def parse_cfg(text: str, **overrides) -> Params:
             kv['alpha'] = float(vals[0])
         elif key in ('x_sym', 'implicit_visc', 'gas_layer_model', 'mr_time_output'):
             flags.add(key)
-        elif key in ('tracers', 'restart_freq', 'output', 'nif_center', 'nif_range',
-                     'gas_layer_data'):
-            if key in ('nif_center', 'nif_range', 'gas_layer_data'):
+        elif key == 'tracers':
+            kv['ntrace'] = int(vals[0])
+        elif key == 'nif_center':
+            kv['nif_mode'] = 1
+        elif key == 'nif_range':
+            kv['nif_mode'], kv['nif_r'] = 2, float(vals[0])
+        elif key in ('restart_freq', 'output', 'gas_layer_data'):
+            if key == 'gas_layer_data':
                 raise OracleError(f"option {key} is outside the restated path")
         else:
             raise OracleError(f"Keyword '{key}' not understood")
@@ -382,7 +406,8 @@ def godunov_set(u0, u1, v0, v1):
 # --------------------------------------------------------------------------
 class Oracle:
     """State and step of fluid_2d + gas_layer_solve (x_sym or not,
-    implicit or explicit viscosity, gas_layer_model, inertial frame)."""
+    implicit or explicit viscosity, gas_layer_model, tracers, inertial or
+    non-inertial frame)."""
 
     def __init__(self, prm: Params):
         self.prm = prm
@@ -401,6 +426,7 @@ class Oracle:
         self.fbd = np.zeros(m); self.pg = np.zeros(m + 1); self.pg_old = np.zeros(m + 1)
         self._solvers = {}
         self.newton_iters = []
+        self.tm = np.zeros(2 * prm.ntrace)   # tracer positions x0, y0, x1, ...
 
     # -------------------------------------------------- index helpers
     def S(self, a, di=0, dj=0):
@@ -428,6 +454,59 @@ class Oracle:
         self.pg[:] = 0
         self.calculate_liquid_fields()
         self.set_boundaries(0.)
+        if prm.ntrace > 0:
+            self.init_tracers()
+
+    def init_tracers(self):
+        """fluid_2d::init_tracers (fluid_2d.cc:495-502) with the C library's
+        rand() of this process (the reference's positions in a process that
+        has not called rand() before)."""
+        import ctypes
+        import ctypes.util
+        libc = ctypes.CDLL(ctypes.util.find_library("c"))
+        rand_max = 2147483647     # glibc RAND_MAX
+        prm = self.prm
+        for k in range(0, self.tm.size, 2):
+            self.tm[k] = prm.ax + (prm.bx - prm.ax) / rand_max * float(libc.rand())
+            self.tm[k + 1] = prm.ay + (prm.by - prm.ay) / rand_max * float(libc.rand())
+
+    def update_tracers(self, dt):
+        """fluid_2d::update_tracers (fluid_2d.cc:507-526): bilinear
+        interpolation of the cell-centred velocity, cell index clamped to
+        [-1, m-1] x [-1, n-1]."""
+        if self.tm.size == 0:
+            return
+        prm = self.prm
+        x = (self.tm[0::2] - prm.ax) * prm.xsp - 0.5
+        y = (self.tm[1::2] - prm.ay) * prm.ysp - 0.5
+        i = np.clip(np.trunc(x).astype(np.int64), -1, self.m - 1)
+        j = np.clip(np.trunc(y).astype(np.int64), -1, self.n - 1)
+        x = x - i
+        y = y - j
+        r, c = j + 2, i + 2
+        for k, f in ((0, self.u), (1, self.v)):
+            val = (1 - y) * (f[r, c] * (1 - x) + f[r, c + 1] * x) + y * (f[r + 1, c] * (1 - x) + f[r + 1, c + 1] * x)
+            self.tm[k::2] += dt * val
+
+    def adjust_frame(self):
+        """fluid_2d::adjust_frame (fluid_2d_sio.cc:228-253)."""
+        prm, m = self.prm, self.m
+        fm = self.v[2, 2:]      # row 0
+        fb = self.v[1, 2:]      # row -1
+        if prm.nif_mode == 1:
+            m2 = m // 2
+            if prm.x_sym:
+                V = 0.5625 * (fb[0] + fm[0]) - 0.0625 * (fb[1] + fm[1])
+            else:
+                V = (0.28125 * (fb[m2 - 1] + fb[m2] + fm[m2 - 1] + fm[m2])
+                     - 0.03125 * (fb[m2 - 2] + fb[m2 + 1] + fm[m2 - 2] + fm[m2 + 1]))
+        else:
+            V = 0.
+            for i in range(prm.nif_a, prm.nif_b):
+                V += float(fm[i]) + float(fb[i])
+            V *= 0.5 / (prm.nif_b - prm.nif_a)
+        self.v -= V
+        self.Vframe -= V
 
     # -------------------------------------------------- gas layer
     def calculate_hx(self):
@@ -683,7 +762,8 @@ class Oracle:
         u, v, p = self.u, self.v, self.p
         shp = u.shape
 
-        # gas layer (fluid_2d.cc:96-102)
+        # tracers (fluid_2d.cc:98), then the gas layer (fluid_2d.cc:96-102)
+        self.update_tracers(dt)
         self.gas_update(dt)
         self.time += 0.5 * dt
 
@@ -840,6 +920,8 @@ class Oracle:
         self.N(p)[:] = z
 
         self.set_viscous_boundaries()
+        if prm.nif_mode:
+            self.adjust_frame()
 
     def _zero_edge(self, E):
         """fluid_2d.cc:480-482."""

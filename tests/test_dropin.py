@@ -48,7 +48,7 @@ def test_host_library_and_driver_built():
     assert os.path.exists(os.path.join(LIB, "vdi_fluid_test"))
 
 
-@pytest.mark.parametrize("extra,msg", [("tracers 5", "Tracers are outside the GPU path"),
+@pytest.mark.parametrize("extra,msg", [("gas_layer_data 64 64 p.dat t.dat", "outside the GPU path"),
                                        ("frobnicate 1", "Keyword 'frobnicate' not understood"),
                                        ("output h bogus", "Output type not understood")])
 def test_config_errors_exit_like_the_reference(tmp_path, extra, msg):
@@ -91,16 +91,21 @@ def _compare_frame(a_dir, b_dir, k):
         assert np.abs(va - vb).max() <= 1e-8 * scale, (name, k)
 
 
-def _restart_parts(path, m, n):
+def _restart_parts(path, m, n, nt=0):
     """The record of fluid_2d_sio.cc:97-119 and gas_layer_solve.cc:323-331:
-    time; u, v, p interleaved over the ghosted grid; Vframe; the gas layer's
-    p[m+1], tau[2..m+1], h[m], ht[m], pg[m+1]."""
+    time; u, v, p interleaved over the ghosted grid; the 2*nt tracer
+    coordinates; Vframe; the gas layer's p[m+1], tau[2..m+1], h[m], ht[m],
+    pg[m+1]."""
     r = np.fromfile(path)
     ng = (m + 4) * (n + 4)
-    assert r.size == 1 + 3 * ng + 1 + (m + 1) + 3 * m + (m + 1)
+    assert r.size == 1 + 3 * ng + 2 * nt + 1 + (m + 1) + 3 * m + (m + 1)
     f = r[1:1 + 3 * ng].reshape(ng, 3)
     o = 1 + 3 * ng
-    parts = {"time": r[:1], "u": f[:, 0], "v": f[:, 1], "p": f[:, 2], "Vframe": r[o:o + 1]}
+    parts = {"time": r[:1], "u": f[:, 0], "v": f[:, 1], "p": f[:, 2]}
+    if nt:
+        parts["tm"] = r[o:o + 2 * nt]
+        o += 2 * nt
+    parts["Vframe"] = r[o:o + 1]
     o += 1
     for k, l in (("gp", m + 1), ("tau", m), ("h", m), ("ht", m), ("pg", m + 1)):
         parts[k] = r[o:o + l]
@@ -108,12 +113,12 @@ def _restart_parts(path, m, n):
     return parts
 
 
-def _compare_restart(a, b, m=256, n=128):
-    pa, pb = _restart_parts(a, m, n), _restart_parts(b, m, n)
+def _compare_restart(a, b, m=256, n=128, nt=0, tol=1e-8):
+    pa, pb = _restart_parts(a, m, n, nt), _restart_parts(b, m, n, nt)
     assert pa["time"][0] == pb["time"][0]
     for k in pb:
         scale = max(float(np.abs(pb[k]).max()), 1e-300)
-        assert np.abs(pa[k] - pb[k]).max() <= 1e-8 * scale, k
+        assert np.abs(pa[k] - pb[k]).max() <= tol * scale, k
 
 
 @pytest.mark.gpu
@@ -157,6 +162,37 @@ def test_fluid_test_frames_and_restarts_match_reference(tmp_path):
         _compare_frame(str(da / "run.odr"), str(db / "run.odr"), k)
     for k in (5, 10):
         _compare_restart(str(da / "run.odr" / f"res.{k}"), str(db / "run.odr" / f"res.{k}"))
+
+
+@pytest.mark.gpu
+def test_fluid_test_tracers_and_moving_frame_match_reference(tmp_path):
+    """fluid_test with 40 tracers and the nif_center frame: the trace.N
+    frames (fluid_2d_sio.cc:121-145), every field frame and the restart
+    records (which carry the tracers) agree with the reference's. Both
+    processes draw the tracers with rand() from its initial state. The
+    frame velocity, taken from four cells each step and subtracted from all
+    of v, carries each step's solver differences (both sides stop at a
+    1e-10 residual) into the next, so over this run's frames the restart
+    records are held to 1e-7 of each field's scale (the 50-step
+    comparisons in test_gpu_step hold 1e-8)."""
+    _need("fluid_test", "fluid_test_b200")
+    da, db = tmp_path / "b200", tmp_path / "ref"
+    txt = _cfg() + "tracers 40\nnif_center\n"
+    for d in (da, db):
+        d.mkdir()
+        (d / "run.cfg").write_text(txt)
+    _run([os.path.join(REF, "fluid_test_b200"), "run.cfg"], str(da))
+    _run([os.path.join(REF, "fluid_test"), "run.cfg"], str(db))
+    for k in range(11):
+        _compare_frame(str(da / "run.odr"), str(db / "run.odr"), k)
+        ta = np.fromfile(str(da / "run.odr" / f"trace.{k}"), dtype=np.float32)
+        tb = np.fromfile(str(db / "run.odr" / f"trace.{k}"), dtype=np.float32)
+        assert ta.size == tb.size == 80
+        assert np.abs(ta.astype(np.float64) - tb).max() <= 2 ** -22 * np.abs(tb).max(), k
+    for k in (5, 10):
+        _compare_restart(str(da / "run.odr" / f"res.{k}"), str(db / "run.odr" / f"res.{k}"), nt=40, tol=1e-7)
+    vf = _restart_parts(str(db / "run.odr" / "res.10"), 256, 128, 40)["Vframe"][0]
+    assert vf < 0.45   # the frame followed the drop
 
 
 @pytest.mark.gpu

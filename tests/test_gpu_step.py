@@ -160,3 +160,72 @@ def test_fused_advection_bit_identical(V, monkeypatch, m, n, drop):
         f.close()
     for k in FIELDS:
         assert np.array_equal(states["1"][k], states["0"][k]), k
+
+
+# ------------------------------------------- tracers and the moving frame
+FRAME = os.path.join(HERE, "golden", "ref_tracers_frame_256x128.npz")
+
+
+@pytest.mark.parametrize("case", ["center", "center_full"])
+def test_tracers_and_frame_match_reference(V, case):
+    """50 steps with tracers and the nif_center frame, with and without
+    x_sym, against the reference run (ref_tracers_frame_256x128.npz):
+    tracer positions and Vframe after 1 and 50 steps, fields after 50."""
+    g = np.load(FRAME)
+    tr = g[f"{case}_trace"]
+    f = V.Fluid2D(str(g[f"{case}_cfg"]), mg_rtol=1e-12, graph=True)
+    f.init_fields()
+    f.set_tracers(tr[0, 2:].reshape(-1, 2))
+    dt = f.frame_dt()
+    span = max(f.prm.bx - f.prm.ax, f.prm.by - f.prm.ay)
+    for k, steps in ((1, 1), (tr.shape[0] - 1, tr.shape[0] - 2)):
+        f.step_forward(dt, steps)
+        st = f.state()
+        assert abs(st["Vframe"] - tr[k, 1]) <= 1e-9 * abs(tr[k, 1]), k
+        assert np.max(np.abs(f.tracers().ravel() - tr[k, 2:])) <= 1e-10 * span, k
+    for fld in ("u", "v", "p"):
+        den = np.max(np.abs(g[f"{case}_s50_{fld}_sub"]))
+        assert np.max(np.abs(st[fld][::4, ::4] - g[f"{case}_s50_{fld}_sub"])) <= TOL * den, fld
+    for fld in ("h", "pg", "gp", "tau", "fbd", "ht"):
+        den = max(np.max(np.abs(g[f"{case}_s50_{fld}"])), 1e-300)
+        assert np.max(np.abs(st[fld] - g[f"{case}_s50_{fld}"])) <= TOL * den, fld
+    assert f.stats()["kernel_launches"] > 0
+
+
+@pytest.mark.parametrize("drop", [(), ("x_sym",)])
+def test_nif_range_and_tracers_match_oracle(V, drop):
+    """The nif_range frame (window of columns, fileinfo.cc:179-191) with 24
+    tracers, 10 steps on both sides from the same tracer positions."""
+    txt = cfg_text(128, 64, drop) + "tracers 24\nnif_range 4e-4\n"
+    o = vo.Oracle(vo.parse_cfg(txt))
+    o.init_fields()
+    f = V.Fluid2D(txt, mg_rtol=1e-12)
+    f.init_fields()
+    f.set_tracers(o.tm.reshape(-1, 2))
+    dt = o.prm.frame_dt()
+    for _ in range(10):
+        o.step(dt)
+    f.step_forward(dt, 10)
+    st = f.state()
+    e = rel_errors(st, o.state())
+    assert max(e.values()) < 1e-9, e
+    assert st["Vframe"] == pytest.approx(o.Vframe, rel=1e-10)
+    assert o.Vframe < o.prm.V
+    span = max(o.prm.bx - o.prm.ax, o.prm.by - o.prm.ay)
+    assert np.max(np.abs(f.tracers().ravel() - o.tm)) <= 1e-12 * span
+
+
+def test_tracer_seeding_matches_reference(V, tmp_path):
+    """init_fields places the tracers with the C library's rand()
+    (fluid_2d.cc:495-502): in a fresh process, exactly the reference's."""
+    import subprocess
+    import sys
+    g = np.load(FRAME)
+    cfg = tmp_path / "c.cfg"
+    cfg.write_text(str(g["center_cfg"]))
+    out = tmp_path / "tm.npy"
+    code = ("import sys, numpy as np; sys.path.insert(0, sys.argv[3]); import vdropimpact_b200 as V; "
+            "f = V.Fluid2D(open(sys.argv[1]).read()); f.init_fields(); np.save(sys.argv[2], f.tracers())")
+    subprocess.run([sys.executable, "-c", code, str(cfg), str(out), os.path.dirname(HERE)], check=True)
+    assert np.array_equal(np.load(out).ravel(), g["center_trace"][0, 2:])
+

@@ -45,6 +45,51 @@ def test_restatement_matches_reference_golden_256x128():
             assert st["time"] == pytest.approx(float(g[f"s{k}_time"]), rel=1e-15)
 
 
+FRAME = os.path.join(GOLD, "ref_tracers_frame_256x128.npz")
+
+
+@pytest.mark.parametrize("case", ["center", "center_full"])
+def test_tracers_and_frame_restatement_matches_reference_golden(case):
+    """50 steps with tracers (fluid_2d.cc:507-526) and the nif_center
+    non-inertial frame (fluid_2d_sio.cc:228-253), with and without x_sym,
+    against the reference run stored in ref_tracers_frame_256x128.npz: the
+    tracer positions and Vframe after every step, the fields after 50."""
+    g = np.load(FRAME)
+    tr = g[f"{case}_trace"]
+    o = vo.Oracle(vo.parse_cfg(str(g[f"{case}_cfg"])))
+    o.init_fields()
+    o.tm[:] = tr[0, 2:]
+    dt = o.prm.frame_dt()
+    span = max(o.prm.bx - o.prm.ax, o.prm.by - o.prm.ay)
+    for k in range(1, tr.shape[0]):
+        o.step(dt)
+        assert o.Vframe == pytest.approx(tr[k, 1], rel=1e-12), k
+        assert np.max(np.abs(o.tm - tr[k, 2:])) <= 1e-13 * span, k
+    st = o.state()
+    for f in ("u", "v", "p"):
+        assert _rel(st[f][::4, ::4], g[f"{case}_s50_{f}_sub"]) < 1e-10, f
+    for f in ("h", "pg", "gp", "tau", "fbd", "ht"):
+        assert _rel(st[f], g[f"{case}_s50_{f}"]) < 1e-10, f
+    assert st["Vframe"] == pytest.approx(float(g[f"{case}_s50_Vframe"]), rel=1e-12)
+    # the frame moved: Vframe fell from V
+    assert tr[-1, 1] < tr[0, 1] - 1e-3
+
+
+def test_tracer_seeding_is_the_references_rand_sequence(tmp_path):
+    """init_tracers draws the positions with the C library's rand()
+    (fluid_2d.cc:495-502): a process that has not called rand() before
+    reproduces the reference's positions exactly."""
+    import sys
+    g = np.load(FRAME)
+    cfg = tmp_path / "c.cfg"
+    cfg.write_text(str(g["center_cfg"]))
+    out = tmp_path / "tm.npy"
+    code = ("import sys, numpy as np; sys.path.insert(0, sys.argv[3]); from oracle import vdi_oracle as vo; "
+            "o = vo.Oracle(vo.parse_cfg(open(sys.argv[1]).read())); o.init_fields(); np.save(sys.argv[2], o.tm)")
+    subprocess.run([sys.executable, "-c", code, str(cfg), str(out), os.path.dirname(HERE)], check=True)
+    assert np.array_equal(np.load(out), g["center_trace"][0, 2:])
+
+
 def test_init_fields_equals_reference_exactly():
     g = np.load(os.path.join(GOLD, "ref_id_vis32_256x128.npz"))
     o = vo.Oracle(vo.parse_cfg(open(os.path.join(GOLD, "id_vis32.cfg")).read()))

@@ -182,6 +182,18 @@ class Fluid2D:
             setattr(st, k, self._ptr(a))
         check(lib().vdi_sim_set_state(self._h, C.byref(st)), "vdi_sim_set_state")
 
+    def tracers(self) -> np.ndarray:
+        """Tracer positions, shape (ntrace, 2): the reference's tm array
+        (fluid_2d.hh:49-50), moved each step by fluid_2d::update_tracers."""
+        out = np.zeros(2 * self.prm.ntrace)
+        check(lib().vdi_sim_get_tracers(self._h, self._ptr(out), out.size), "vdi_sim_get_tracers")
+        return out.reshape(-1, 2)
+
+    def set_tracers(self, xy):
+        """Places the tracers (ntrace x 2 positions)."""
+        a = np.ascontiguousarray(xy, dtype=np.float64).ravel()
+        check(lib().vdi_sim_set_tracers(self._h, self._ptr(a), a.size), "vdi_sim_set_tracers")
+
     def stats(self, reset: bool = False) -> dict:
         s = _abi.VdiStats()
         check(lib().vdi_sim_stats(self._h, C.byref(s), int(reset)), "vdi_sim_stats")

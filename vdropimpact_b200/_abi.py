@@ -50,7 +50,8 @@ class VdiParams(C.Structure):
                 ("alpha", C.c_double), ("mug", C.c_double), ("Pamb", C.c_double), ("h0", C.c_double),
                 ("R", C.c_double), ("V", C.c_double), ("sigma", C.c_double),
                 ("mg_rtol", C.c_double), ("mg_max_vcycles", C.c_int), ("mg_precision", C.c_int),
-                ("mg_guess", C.c_int)]
+                ("mg_guess", C.c_int),
+                ("ntrace", C.c_int), ("nif_mode", C.c_int), ("nif_a", C.c_int), ("nif_b", C.c_int)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -116,6 +117,8 @@ _SIGS = [
     ("vdi_sim_synchronize", C.c_int, [C.c_void_p]),
     ("vdi_sim_get_state", C.c_int, [C.c_void_p, C.POINTER(VdiState)]),
     ("vdi_sim_set_state", C.c_int, [C.c_void_p, C.POINTER(VdiState)]),
+    ("vdi_sim_get_tracers", C.c_int, [C.c_void_p, _dp, C.c_long]),
+    ("vdi_sim_set_tracers", C.c_int, [C.c_void_p, _dp, C.c_long]),
     ("vdi_sim_stats", C.c_int, [C.c_void_p, C.POINTER(VdiStats), C.c_int]),
     ("vdi_sim_device_field", C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(C.c_size_t)]),
     ("vdi_sim_autotune", C.c_int, [C.c_void_p, C.POINTER(VdiTune)]),

@@ -51,6 +51,8 @@ struct vdi_sim {
     GuessHist* hist = nullptr;   // 4 entries
     double* d_time = nullptr;
     double* d_vframe = nullptr;
+    double* d_tm = nullptr;     // tracer positions x0, y0, x1, ... (2 * ntrace)
+    double* d_vacc = nullptr;   // the non-inertial frame's velocity of a step
     int* d_err = nullptr;
     GasStats* d_gstats = nullptr;
     MG* mg[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -128,6 +130,9 @@ int enqueue_step(vdi_sim* S, double dt) {
     // clock, so the FEM guess has read it by then.
     VDI_CUDA(cudaEventRecord(S->ev_fork, s));
     VDI_CUDA(cudaStreamWaitEvent(S->s_gas, S->ev_fork, 0));
+    // tracers first (fluid_2d.cc:98), before anything rewrites u, v or
+    // their ghost cells
+    VDI_TRY(launch_tracers(s, g, S->f, S->d_tm, S->prm.ntrace, dt));
     VDI_TRY(launch_gas_update(S->s_gas, S->gp, S->gas, S->f.u, S->f.v, m + 4, S->d_vframe, dt, S->d_time,
                               S->gas_work, S->d_err, S->d_gstats));
     // h is final for this step once the gas layer has updated it
@@ -197,6 +202,9 @@ int enqueue_step(vdi_sim* S, double dt) {
     VDI_TRY(mg_solve_device(S->mg[SOLVER_FEM], s, S->src_fem, S->zf, prec));
     VDI_TRY(launch_vel_update(s, g, S->f, c0v, c1v, S->zf, dt));
     VDI_TRY(launch_viscous_bc(s, g, S->f, S->gas));
+    // the non-inertial frame last (fluid_2d.cc:404)
+    if (S->prm.nif_mode != 0)
+        VDI_TRY(launch_frame(s, g, S->f, S->prm.nif_mode, S->prm.nif_a, S->prm.nif_b, S->d_vacc, S->d_vframe));
     return VDI_OK;
 }
 
@@ -259,7 +267,8 @@ int parse_cfg(const char* text, vdi_params* P) {
     int m = -1, n = -1, nframes = -1, glo = 0;
     double L_nd = -1, h0_nd = -1, t_end_nd = -1, tmult = -1, nul = -1, rho = -1, R = -1, V = -1, alpha = -1,
            sigma = -1, mug = -1, Pamb = -1;
-    int x_sym = 0, implicit_visc = 0;
+    int x_sym = 0, implicit_visc = 0, ntrace = 0, nif_mode = 0;
+    double nif_r = 0;
     std::istringstream in(text);
     std::string line;
     int ln = 0;
@@ -298,8 +307,13 @@ int parse_cfg(const char* text, vdi_params* P) {
         else if (key == "x_sym") x_sym = 1;
         else if (key == "implicit_visc") implicit_visc = 1;
         else if (key == "gas_layer_model") glo = 2;
-        else if (key == "mr_time_output" || key == "tracers" || key == "restart_freq" || key == "output") {
-        } else if (key == "gas_layer_data" || key == "nif_center" || key == "nif_range") {
+        else if (key == "tracers") ntrace = atoi(vals.empty() ? "-1" : vals[0].c_str());
+        else if (key == "nif_center") nif_mode = 1;                 // fileinfo.cc:96-98
+        else if (key == "nif_range") {                              // fileinfo.cc:99-101
+            nif_mode = 2;
+            nif_r = num(0);
+        } else if (key == "mr_time_output" || key == "restart_freq" || key == "output") {
+        } else if (key == "gas_layer_data") {
             set_error("option '%s' is outside the GPU path (line %d)", key.c_str(), ln);
             return VDI_ERR_CONFIG;
         } else {
@@ -331,6 +345,26 @@ int parse_cfg(const char* text, vdi_params* P) {
     P->mg_max_vcycles = 200;
     P->mg_precision = VDI_MG_FP64;
     P->mg_guess = VDI_GUESS_EXTRAPOLATE;
+    if (ntrace < 0) { set_error("Value of tracers invalid"); return VDI_ERR_CONFIG; }
+    P->ntrace = ntrace;
+    P->nif_mode = nif_mode;
+    if (nif_mode == 2) {
+        // fileinfo.cc:179-191: the columns whose centres lie within nif_r
+        const double xsp = 1. / ((P->bx - P->ax) / m);
+        int b = int((nif_r - P->ax) * xsp + 0.5), a;
+        if (b >= m) b = m - 1;
+        if (x_sym) a = 0;
+        else {
+            a = int((-nif_r - P->ax) * xsp + 0.5);
+            if (a < 0) a = 0;
+        }
+        if (b - a <= 0) {
+            set_error("Velocity window for non-inertial frame is too small");
+            return VDI_ERR_CONFIG;
+        }
+        P->nif_a = a;
+        P->nif_b = b;
+    }
     return VDI_OK;
 }
 
@@ -370,7 +404,7 @@ int parse_run_options(const char* text, vdi_run_options* O) {
                 }
                 O->fflags |= 1u << k;
             }
-        } else if (key == "gas_layer_data" || key == "nif_center" || key == "nif_range") {
+        } else if (key == "gas_layer_data") {
             set_error("option '%s' is outside the GPU path (line %d)", key.c_str(), ln);
             return VDI_ERR_CONFIG;
         }
@@ -422,6 +456,11 @@ int vdi_params_from_cfg(const char* cfg_text, vdi_params* out) {
 int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     if (!prm || !out || prm->m < 4 || prm->n < 4) {
         set_error("vdi_sim_create: invalid parameters");
+        return VDI_ERR_INVALID_ARGUMENT;
+    }
+    if (prm->ntrace < 0 || prm->nif_mode < 0 || prm->nif_mode > 2 ||
+        (prm->nif_mode == 2 && !(prm->nif_a >= 0 && prm->nif_a < prm->nif_b && prm->nif_b <= prm->m))) {
+        set_error("vdi_sim_create: invalid tracer or non-inertial frame parameters");
         return VDI_ERR_INVALID_ARGUMENT;
     }
     vdi_sim* S = new vdi_sim();
@@ -499,6 +538,8 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     S->d_time = misc;
     S->d_vframe = misc + 1;
     S->hist = reinterpret_cast<GuessHist*>(misc + 2);
+    if (P.ntrace > 0 && (st = alloc_zero(S, &S->d_tm, 2 * size_t(P.ntrace))) != VDI_OK) return fail(st);
+    if (P.nif_mode != 0 && (st = alloc_zero(S, &S->d_vacc, 1)) != VDI_OK) return fail(st);
     double* ebuf;
     if ((st = alloc_zero(S, &ebuf, 1 + sizeof(GasStats) / 8 + 1)) != VDI_OK) return fail(st);
     S->d_err = reinterpret_cast<int*>(ebuf);
@@ -616,7 +657,34 @@ int vdi_sim_init_fields(vdi_sim* S) {
     VDI_TRY(launch_inviscid_bc(s, S->g, S->f, S->gas, 0.));
     VDI_TRY(launch_viscous_bc(s, S->g, S->f, S->gas));
     VDI_TRY(liftoff_restart(S));
+    if (S->prm.ntrace > 0) {
+        // fluid_2d::init_tracers (fluid_2d.cc:495-502): the process's rand()
+        const vdi_params& P = S->prm;
+        std::vector<double> tm(2 * size_t(P.ntrace));
+        for (size_t k = 0; k < tm.size(); k += 2) {
+            tm[k] = P.ax + (P.bx - P.ax) / RAND_MAX * static_cast<double>(rand());
+            tm[k + 1] = P.ay + (P.by - P.ay) / RAND_MAX * static_cast<double>(rand());
+        }
+        VDI_CUDA(cudaMemcpyAsync(S->d_tm, tm.data(), tm.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        VDI_CUDA(cudaStreamSynchronize(s));
+    }
     VDI_CUDA(cudaStreamSynchronize(s));
+    return VDI_OK;
+}
+
+int vdi_sim_get_tracers(vdi_sim* S, double* h_xy, long count) {
+    if (!S || (count > 0 && !h_xy) || count != 2L * S->prm.ntrace) return VDI_ERR_INVALID_ARGUMENT;
+    if (count == 0) return VDI_OK;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    VDI_CUDA(cudaMemcpy(h_xy, S->d_tm, size_t(count) * sizeof(double), cudaMemcpyDeviceToHost));
+    return VDI_OK;
+}
+
+int vdi_sim_set_tracers(vdi_sim* S, const double* h_xy, long count) {
+    if (!S || (count > 0 && !h_xy) || count != 2L * S->prm.ntrace) return VDI_ERR_INVALID_ARGUMENT;
+    if (count == 0) return VDI_OK;
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    VDI_CUDA(cudaMemcpy(S->d_tm, h_xy, size_t(count) * sizeof(double), cudaMemcpyHostToDevice));
     return VDI_OK;
 }
 
@@ -787,9 +855,11 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     // and the final boundary kernel (+1 viscous source when implicit); per
     // solve the initial guess and the start check; per solve-loop iteration
     // the kernels of its V-cycle;
-    // per step the lift-off search when it is on, and with the learned guess
-    // the residual kernel and the network's correction.
+    // per step the lift-off search when it is on, the tracers and the two
+    // frame kernels when those are on, and with the learned guess the
+    // residual kernel and the network's correction.
     long per_step = 11 - (S->fused_advect ? 2 : 0) + (S->prm.implicit_visc ? 1 : 0) + (S->lcfg.mode != VDI_LIFTOFF_OFF ? 1 : 0) +
+                    (S->prm.ntrace > 0 ? 1 : 0) + (S->prm.nif_mode != 0 ? 2 : 0) +
                     (S->prm.mg_guess == VDI_GUESS_LEARNED ? 1 + unet_kernels_per_correction() : 0);
     long launches = S->steps * per_step;
     for (int k = 0; k < 4; k++) {

@@ -8,6 +8,8 @@
 // reference's double-precision results bit for bit.
 #include "step_kernels.hh"
 
+#include <algorithm>
+
 #include <cmath>
 
 namespace vdi {
@@ -632,6 +634,61 @@ __global__ void k_vel_update(Grid g, Fields f, CellView c0v, CellView c1v, const
     }
 }
 
+// ------------------------------------------------------------- tracers
+// fluid_2d::update_tracers (fluid_2d.cc:507-526): each tracer moves by dt
+// times the bilinear interpolation of the cell-centred velocity around it,
+// the cell index clamped to [-1, m-1] x [-1, n-1] (ghost cells included).
+__global__ void k_tracers(Grid g, const double* __restrict__ u, const double* __restrict__ v,
+                          double* __restrict__ tm, int ntrace, double dt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntrace) return;
+    double* tp = tm + 2 * t;
+    double x = (tp[0] - g.ax) * g.xsp - 0.5, y = (tp[1] - g.ay) * g.ysp - 0.5;
+    int i = int(x);
+    if (i < -1) i = -1;
+    if (i > g.m - 1) i = g.m - 1;
+    int j = int(y);
+    if (j < -1) j = -1;
+    if (j > g.n - 1) j = g.n - 1;
+    x -= i;
+    y -= j;
+    const int P = g.m + 4, c = (j + 2) * P + i + 2;
+    tp[0] += dt * ((1 - y) * (u[c] * (1 - x) + u[c + 1] * x) + y * (u[c + P] * (1 - x) + u[c + P + 1] * x));
+    tp[1] += dt * ((1 - y) * (v[c] * (1 - x) + v[c + 1] * x) + y * (v[c + P] * (1 - x) + v[c + P + 1] * x));
+}
+
+// ------------------------------------------------- non-inertial frame
+// fluid_2d::adjust_frame (fluid_2d_sio.cc:228-253): the frame velocity from
+// the two rows around the liquid's bottom edge (row -1 and row 0), either a
+// Lagrange interpolant at the centre (mode 1) or the mean over columns
+// [a, b) summed in column order (mode 2); one thread, so the sum's order is
+// the reference's.
+__global__ void k_frame_velocity(Grid g, const double* __restrict__ v, int mode, int a, int b, double* vacc) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int P = g.m + 4;
+    const double* fm = v + 2 * P + 2;
+    const double* fb = fm - P;
+    double V;
+    if (mode == 1) {
+        const int m2 = g.m / 2;
+        V = g.x_sym ? 0.5625 * (fb[0] + fm[0]) - 0.0625 * (fb[1] + fm[1])
+                    : 0.28125 * (fb[m2 - 1] + fb[m2] + fm[m2 - 1] + fm[m2]) -
+                          0.03125 * (fb[m2 - 2] + fb[m2 + 1] + fm[m2 - 2] + fm[m2 + 1]);
+    } else {
+        V = 0;
+        for (int i = a; i < b; i++) V += fm[i] + fb[i];
+        V *= 0.5 / (b - a);
+    }
+    *vacc = V;
+}
+/** Subtracts the frame velocity from v over the whole ghosted grid and from
+ * the gas layer's Vframe. */
+__global__ void k_frame_apply(double* __restrict__ v, long tot, const double* __restrict__ vacc, double* vframe) {
+    const double V = *vacc;
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) v[k] -= V;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *vframe -= V;
+}
+
 // ------------------------------------------------ multigrid initial guess
 // mgs_common::initial_guess (mgs_common.cc:17-50). The decision is made from
 // device-resident times so that a captured graph replays it correctly. One
@@ -779,6 +836,19 @@ int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c
     k_vel_update<<<cell_grid(g, 1), cell_block(g), 0, s>>>(g, f, c0, c1, z, dt);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
+int launch_tracers(cudaStream_t s, const Grid& g, const Fields& f, double* tm, int ntrace, double dt) {
+    if (ntrace <= 0) return VDI_OK;
+    k_tracers<<<(ntrace + 127) / 128, 128, 0, s>>>(g, f.u, f.v, tm, ntrace, dt);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+int launch_frame(cudaStream_t s, const Grid& g, const Fields& f, int mode, int a, int b, double* vacc,
+                 double* vframe) {
+    const long tot = long(g.m + 4) * (g.n + 4);
+    k_frame_velocity<<<1, 32, 0, s>>>(g, f.v, mode, a, b, vacc);
+    k_frame_apply<<<int(std::min<long>((tot + 255) / 256, 1184)), 256, 0, s>>>(f.v, tot, vacc, vframe);
+    return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
+}
+
 int launch_guess(cudaStream_t s, double* z, double* zprev, double* zprev2, int n, GuessHist* h,
                  const double* d_time, double tadd, int quadratic, int* err) {
     if (n <= 0) return VDI_OK;

@@ -82,6 +82,12 @@ int launch_fem_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs
                    double a_cc_edge, double a_cc_mid, double* src);
 int launch_vel_update(cudaStream_t s, const Grid& g, const Fields& f, CellView c0, CellView c1, const double* z,
                       double dt);
+/** fluid_2d::update_tracers (fluid_2d.cc:507-526) for ntrace tracers. */
+int launch_tracers(cudaStream_t s, const Grid& g, const Fields& f, double* tm, int ntrace, double dt);
+/** fluid_2d::adjust_frame (fluid_2d_sio.cc:228-253): mode 1 (nif_center) or
+ * 2 (nif_range over columns [a, b)); vacc is a device scratch double. */
+int launch_frame(cudaStream_t s, const Grid& g, const Fields& f, int mode, int a, int b, double* vacc,
+                 double* vframe);
 /** One launch of the initial guess at time *d_time + tadd: the reference's
  * linear rule, or (quadratic != 0) quadratic-in-time extrapolation from the
  * last three solutions (zprev2 the oldest, unused by the linear rule), which

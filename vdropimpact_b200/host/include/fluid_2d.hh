@@ -35,7 +35,8 @@ class fluid_2d : public fileinfo {
         field* const fbase;
         /** The (0,0) cell of fbase. */
         field* const fm;
-        /** Tracer positions (none on the GPU path). */
+        /** Tracer positions x0, y0, x1, ... (2*ntrace; host copy of the
+         * device's, refreshed by sync_fields). */
         double* const tm;
         /** A host source array of the node grid (me*ne), the right-hand side
          * that a standalone visco_impl bound to this object solves with. */
@@ -53,6 +54,7 @@ class fluid_2d : public fileinfo {
         void write_files(int k);
         void output(const char* prefix, const int mode, int sn, bool ghost = false);
         void output_pbase_full(int sn);
+        void output_tracers(int sn);
         inline int timestep_select(double interval, double& adt) {
             int l = static_cast<int>(interval / dt_reg) + 1;
             adt = interval / l;

@@ -34,11 +34,11 @@ fileinfo::fileinfo(const char* infile)
     int st = vdi_params_from_cfg(text.c_str(), &params);
     if (st == VDI_OK) st = vdi_run_options_from_cfg(text.c_str(), &ro);
     if (st != VDI_OK) fatal_error(vdi_last_error(), 1);
-    if (ro.ntrace > 0) fatal_error("Tracers are outside the GPU path", 1);
     m = params.m;
     n = params.n;
     fflags = ro.fflags;
-    ntrace = ro.ntrace;
+    ntrace = params.ntrace;
+    nif_mode = params.nif_mode;
     nframes = params.nframes;
     restart_freq = ro.restart_freq;
     implicit_visc = params.implicit_visc != 0;

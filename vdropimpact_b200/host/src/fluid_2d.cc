@@ -12,7 +12,7 @@ fluid_2d::fluid_2d(const char* infile)
     : fileinfo(infile), mn(m * n), me(m + 1), ne(n + 1), ml(m + 4), dx((bx - ax) / m), dy((by - ay) / n),
       xsp(1. / dx), ysp(1. / dy), xxsp(xsp * xsp), yysp(ysp * ysp),
       dt_reg(implicit_visc ? dx * tmult : dx * dx * rho * muinv * tmult * 0.25),
-      fbase(new field[ml * (n + 4)]()), fm(fbase + 2 * ml + 2), tm(new double[2]()), src(new double[me * ne]()),
+      fbase(new field[ml * (n + 4)]()), fm(fbase + 2 * ml + 2), tm(new double[2 * ntrace + 2]()), src(new double[me * ne]()),
       time(0.), f_num(0), S(NULL), buf(new float[m > 123 ? m + 5 : 128]) {
     vdi_check(vdi_sim_create(&params, NULL, &S), "vdi_sim_create");
     vdi_check(vdi_sim_use_graph(S, 1), "vdi_sim_use_graph");
@@ -95,6 +95,7 @@ void fluid_2d::sync_fields() {
     s.pg = g->pg;
     s.ht = g->ht;
     vdi_check(vdi_sim_get_state(S, &s), "vdi_sim_get_state");
+    vdi_check(vdi_sim_get_tracers(S, tm, 2L * ntrace), "vdi_sim_get_tracers");
     for (int k = 0; k < tot; k++) {
         fbase[k].u = u[k];
         fbase[k].v = v[k];
@@ -127,6 +128,7 @@ void fluid_2d::push_fields() {
     s.pg = g->pg;
     s.ht = g->ht;
     vdi_check(vdi_sim_set_state(S, &s), "vdi_sim_set_state");
+    vdi_check(vdi_sim_set_tracers(S, tm, 2L * ntrace), "vdi_sim_set_tracers");
 }
 
 void fluid_2d::load_restart(int sn) {
@@ -201,7 +203,20 @@ void fluid_2d::write_files(int k) {
     if (fflags & 512) gl->output_profile_double(filename, buf, k, 0);
     if (fflags & 1024) gl->output_profile_double(filename, buf, k, 1);
     if (fflags & 2048) gl->output_profile_double(filename, buf, k, 2);
+    if (ntrace > 0) output_tracers(k);
     if (restart_freq > 0 && k > 0 && k % restart_freq == 0) save_restart(k);
+}
+
+void fluid_2d::output_tracers(const int sn) {
+    // fluid_2d_sio.cc:121-145: the 2*ntrace coordinates as floats
+    FILE* outf = odir_open("trace", sn, "wb");
+    const int tot = ntrace << 1;
+    for (int j = 0; j < tot; j += 128) {
+        const int c = tot - j < 128 ? tot - j : 128;
+        for (int q = 0; q < c; q++) buf[q] = float(tm[j + q]);
+        fwrite(buf, sizeof(float), c, outf);
+    }
+    fclose(outf);
 }
 
 void fluid_2d::output_pbase_full(const int sn) {
