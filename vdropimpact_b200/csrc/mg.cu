@@ -267,18 +267,25 @@ __device__ __forceinline__ T cc_interp(const CCc<T>& f, const TC* zc, int i, int
     return cc_interp_rows(f, [&](int J) { return zc + mc * J; }, i, j);
 }
 
-/** Bilinear prolongation of node-centred corrections to fine node (i,j). */
-template <typename T, typename TC>
-__device__ __forceinline__ T fem_interp(const FEMc<T>& f, const TC* zc, int i, int j) {
+/** Bilinear prolongation of node-centred corrections to fine node (i,j);
+ * row(J) gives coarse node row J (indexable by the coarse column). */
+template <typename T, class ROW>
+__device__ __forceinline__ T fem_interp_rows(const FEMc<T>& f, ROW row, int i, int j) {
     if (j == 0) return T(0);
-    const int Mc = (f.M - 1) / 2 + 1;
     int I = i >> 1, J = j >> 1;
     bool ox = i & 1, oy = j & 1;
-    T c00 = T(zc[I + Mc * J]);
+    const auto* r0 = row(J);
+    T c00 = T(r0[I]);
     if (!ox && !oy) return c00;
-    if (ox && !oy) return T(0.5) * (c00 + T(zc[I + 1 + Mc * J]));
-    if (!ox && oy) return T(0.5) * (c00 + T(zc[I + Mc * (J + 1)]));
-    return T(0.25) * (c00 + T(zc[I + 1 + Mc * J]) + T(zc[I + Mc * (J + 1)]) + T(zc[I + 1 + Mc * (J + 1)]));
+    if (ox && !oy) return T(0.5) * (c00 + T(r0[I + 1]));
+    const auto* r1 = row(J + 1);
+    if (!ox && oy) return T(0.5) * (c00 + T(r1[I]));
+    return T(0.25) * (c00 + T(r0[I + 1]) + T(r1[I]) + T(r1[I + 1]));
+}
+template <typename T, typename TC>
+__device__ __forceinline__ T fem_interp(const FEMc<T>& f, const TC* zc, int i, int j) {
+    const int Mc = (f.M - 1) / 2 + 1;
+    return fem_interp_rows(f, [&](int J) { return zc + Mc * J; }, i, j);
 }
 
 /** P^T r at coarse node (I,J) from a residual array with origin (ox,oy) and
@@ -459,7 +466,37 @@ __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<
                 bool in = unsigned(i) < unsigned(m) && unsigned(j) < unsigned(n);
                 zv[q][h] = (in && read_z) ? a.zin[i + m * j] : T(0);
                 bv[q][h] = in ? a.b[i + m * j] : T(0);
-                if (MODE == 1 && in) zv[q][h] += cc_interp(c, a.zc, i, j);
+            }
+        }
+        if constexpr (MODE == 1) {
+            // POST: the coarse correction of the window (coarse columns and
+            // rows (zx>>1)-1 .. ((zx+63)>>1)+1, 35 of each since the window
+            // origin is odd) staged in shared memory, then prolonged from there
+            constexpr int CC = CW / 2 + 3;
+            static_assert(CC == CH / 2 + 3, "square window");
+            __shared__ TC cwin[CC * CC];
+            const int mc = m >> 1, nc = n >> 1, I0 = (zx >> 1) - 1, J0 = (zy >> 1) - 1;
+            constexpr int PER = (CC * CC + G::NT - 1) / G::NT;
+            TC cv[PER];
+#pragma unroll
+            for (int u = 0; u < PER; u++) {
+                const int k = threadIdx.x + u * G::NT, Jl = k / CC, I = I0 + (k - Jl * CC), J = J0 + Jl;
+                cv[u] = (k < CC * CC && unsigned(I) < unsigned(mc) && unsigned(J) < unsigned(nc)) ? a.zc[I + mc * J]
+                                                                                                 : TC(0);
+            }
+#pragma unroll
+            for (int u = 0; u < PER; u++)
+                if (threadIdx.x + u * G::NT < CC * CC) cwin[threadIdx.x + u * G::NT] = cv[u];
+            __syncthreads();
+            auto row = [&](int J) { return cwin + (J - J0) * CC - I0; };
+#pragma unroll
+            for (int q = 0; q < RPW; q++) {
+                const int j = zy + warp + q * NW;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int i = zx + lane + 32 * h;
+                    if (unsigned(i) < unsigned(m) && unsigned(j) < unsigned(n)) zv[q][h] += cc_interp_rows(c, row, i, j);
+                }
             }
         }
 #pragma unroll
@@ -545,7 +582,37 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
                 bool in = unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N);
                 zv[q][h] = (in && read_z) ? a.zin[i + M * j] : T(0);
                 bv[q][h] = in ? a.b[i + M * j] : T(0);
-                if (MODE == 1 && in) zv[q][h] += fem_interp(c, a.zc, i, j);
+            }
+        }
+        if constexpr (MODE == 1) {
+            // POST: the coarse correction of the window (coarse nodes
+            // zx/2 .. zx/2+32 by zy/2 .. zy/2+32; the window origin is even)
+            // staged in shared memory, then prolonged from there
+            constexpr int CC = G::CW / 2 + 1;
+            static_assert(CC == CH / 2 + 1, "square window");
+            __shared__ TC cwin[CC * CC];
+            const int Mc = (M - 1) / 2 + 1, Nc = (N - 1) / 2 + 1, I0 = zx >> 1, J0 = zy >> 1;
+            constexpr int PER = (CC * CC + G::NT - 1) / G::NT;
+            TC cv[PER];
+#pragma unroll
+            for (int u = 0; u < PER; u++) {
+                const int k = threadIdx.x + u * G::NT, Jl = k / CC, I = I0 + (k - Jl * CC), J = J0 + Jl;
+                cv[u] = (k < CC * CC && unsigned(I) < unsigned(Mc) && unsigned(J) < unsigned(Nc)) ? a.zc[I + Mc * J]
+                                                                                                 : TC(0);
+            }
+#pragma unroll
+            for (int u = 0; u < PER; u++)
+                if (threadIdx.x + u * G::NT < CC * CC) cwin[threadIdx.x + u * G::NT] = cv[u];
+            __syncthreads();
+            auto row = [&](int J) { return cwin + (J - J0) * CC - I0; };
+#pragma unroll
+            for (int q = 0; q < RPW; q++) {
+                const int j = zy + warp + q * NW;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int i = zx + lane + 32 * h;
+                    if (unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N)) zv[q][h] += fem_interp_rows(c, row, i, j);
+                }
             }
         }
 #pragma unroll
