@@ -356,10 +356,12 @@ __device__ __forceinline__ void cc_window_phases(const CCc<T>& c, T* Z, const T*
 #pragma unroll
         for (int q = 0; q < RPW; q++) {
             const int jj = warp + q * NW;
-            if (jj < 1 || jj > CH - 2) continue;
+            // phase ph can only be exact at ph+1 or more cells from the
+            // window's edge (its neighbours nearer the edge are stale)
+            if (jj < ph + 1 || jj > CH - 2 - ph) continue;
             const int p = (color ^ par0 ^ jj) & 1;
             const int ii = 2 * lane + p;
-            if (ii == 0 || ii == CW - 1) continue;
+            if (ii < ph + 1 || ii > CW - 2 - ph) continue;
             const T* zo = Zo + jj * KW;
             const T l = zo[lane - 1 + p], r = zo[lane + p];
             const T d = Zo[(jj - 1) * KW + lane], u = Zo[(jj + 1) * KW + lane];
@@ -640,7 +642,9 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
         for (int q = 0; q < QW / NW; q++) {
             const int jr = warp + q * NW, ir = lane;
             const int ii = 2 * ir + ci, jj = 2 * jr + cj;
-            if (ii == 0 || ii == G::CW - 1 || jj == 0 || jj == CH - 1) continue;
+            // phase ph can only be exact at ph+1 or more cells from the
+            // window's edge (its neighbours nearer the edge are stale)
+            if (ii < ph + 1 || ii > G::CW - 2 - ph || jj < ph + 1 || jj > CH - 2 - ph) continue;
             const int xl = ir - 1 + ci, xr = ir + ci, yd = jr - 1 + cj, yu = jr + cj;
             const T l = Zx[jr * QW + xl], r = Zx[jr * QW + xr];
             const T d = Zy[yd * QW + ir], u = Zy[yu * QW + ir];
