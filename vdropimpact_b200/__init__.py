@@ -340,6 +340,38 @@ def sweep_configs(count: int, seed: int = 0, sizes=(256, 512, 1024)):
     return out
 
 
+def sweep_cost(cfg: str) -> float:
+    """Relative cost of running one .cfg to its end: cells times timesteps
+    (the frame interval over the timestep of fluid_2d.hh:82-86, times the
+    frames)."""
+    p = params_from_cfg(cfg)
+    dx = (p.bx - p.ax) / p.m
+    rho, mu = p.rho, p.mu
+    dt_reg = dx * p.tmult if p.implicit_visc else dx * dx * rho / mu * p.tmult * 0.25
+    steps_per_frame = int((p.t_end / p.nframes) / dt_reg) + 1
+    return float(p.m) * p.n * steps_per_frame * p.nframes
+
+
+def shard_sweep(cfgs, rank: int, world: int):
+    """The indices of the simulations of a sweep that rank `rank` of `world`
+    runs: longest first onto the least-loaded rank (ties to the lower rank),
+    by sweep_cost. Every rank computes the same assignment from the same
+    list, so ranks need no exchange; the simulations are independent and a
+    rank runs its share as one Batch."""
+    if not (0 <= rank < world):
+        raise ValueError("rank must lie in [0, world)")
+    costs = [sweep_cost(c) for c in cfgs]
+    order = sorted(range(len(cfgs)), key=lambda k: (-costs[k], k))
+    load = [0.0] * world
+    mine = []
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += costs[k]
+        if r == rank:
+            mine.append(k)
+    return sorted(mine)
+
+
 def profile_min(h, ax: float, dx: float, mode: str = "smoothed"):
     """(x, height) of the minimum of one height profile (a float64 CUDA
     tensor of m cell values) as the reference's analysis tool finds it
