@@ -256,9 +256,9 @@ def measured_peak_gbs():
 
 
 # DRAM bytes (read + write) of one launch of the roofline kernel, from the ncu
-# capture summarised in profiles/cc_tile_post_fp64_4096x2048.md (192.6 MB at
+# capture summarised in profiles/cc_tile_post_fp64_4096x2048.md (196.3 MB at
 # 4096x2048), scaled to the 2048x1024 bench grid by the number of cells.
-CC_POST_DRAM_BYTES = 192.6e6 / 4
+CC_POST_DRAM_BYTES = 196.3e6 / 4
 
 
 def roofline(V, torch, args):
