@@ -78,3 +78,15 @@ def test_shard_sweep_single_rank_and_bad_rank():
     assert V.shard_sweep(cfgs, 0, 1) == list(range(7))
     with pytest.raises(ValueError):
         V.shard_sweep(cfgs, 2, 2)
+
+
+def test_sweep_cost_is_cells_times_the_references_timesteps():
+    """sweep_cost counts the timesteps fluid_2d::solve takes
+    (fluid_2d.hh:82-86, fluid_2d.cc:42), as the oracle restates them."""
+    sys.path.insert(0, ROOT)
+    from oracle import vdi_oracle as vo
+    import vdropimpact_b200 as V
+    for cfg in V.sweep_configs(12, seed=9):
+        p = vo.parse_cfg(cfg)
+        l, _ = p.timestep_select(p.t_end / p.nframes)
+        assert V.sweep_cost(cfg) == float(p.m * p.n * l * p.nframes)
