@@ -176,10 +176,10 @@ def run_reference_arm(args, ws, rank):
         return
     text = cfg_text(args.grid)
     # each "step" of this arm is one reference timestep; the run times
-    # args.steps of them after args.warmup untimed ones, capped so the whole
-    # run stays within a few minutes
-    steps = max(1, min(args.steps, 20))
-    warm = max(1, min(args.warmup, 3))
+    # args.steps of them after args.warmup untimed ones, the same window as
+    # the GPU arm (about 0.15 s per step on 16 host cores at 2048x1024)
+    steps = max(1, args.steps)
+    warm = max(0, args.warmup)
     r = cpu_reference(text, steps, warm)
     if "unavailable" in r:
         print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
@@ -255,9 +255,9 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) of one launch of the roofline kernel, from the ncu
-# capture summarised in profiles/cc_tile_post_fp64_4096x2048.md (196.3 MB at
-# 4096x2048), scaled to the 2048x1024 bench grid by the number of cells.
+# DRAM bytes (read + write) of one launch of the roofline kernel, from an ncu
+# capture of the same kernel on a 4096x2048 grid (196.3 MB per launch),
+# scaled to the 2048x1024 bench grid by the number of cells.
 CC_POST_DRAM_BYTES = 196.3e6 / 4
 
 
@@ -277,6 +277,98 @@ def roofline(V, torch, args):
     return {"kernel": "cc_tile<double, POST> on the 2048x1024 MAC grid", "bound": "hbm", "achieved": achieved,
             "peak": peak, "peak_source": kind, "unit": "GB/s", "frac": achieved / peak,
             "traffic": CC_POST_DRAM_BYTES, "algorithmic_bytes": nbytes, "ms_per_launch": ms}
+
+
+# Canonical algorithmic bytes of the step's work outside the multigrid
+# V-cycles, per liquid cell, 8-byte words: advection to the MAC source 10,
+# MAC correction and advective update 11, two viscous sources 4, FEM source
+# 3, velocity/pressure update 6 (34 words); and per point of each solve the
+# time-extrapolated initial guess (4 words).
+STEP_WORDS_PER_CELL = 34
+GUESS_WORDS_PER_POINT = 4
+
+
+def canonical_step(f, res, peak):
+    """Step-level roofline with canonical bytes: the non-multigrid work, the
+    guesses, and every V-cycle taken in the timed window at its hierarchy's
+    canonical bytes per iteration."""
+    st = res["stats"]
+    steps = max(st["steps"], 1)
+    per_iter = res["vcycle_bytes"]
+    cells = f.m * f.n
+    pts = {"MAC": cells, "FEM": (f.m + 1) * (f.n + 1), "VX": cells, "VY": cells}
+    mg = sum(st["vcycles"][k] * per_iter[k] for k in per_iter) / steps
+    guess = sum(st["solves"][k] * pts[k] for k in pts) * GUESS_WORDS_PER_POINT * 8 / steps
+    other = STEP_WORDS_PER_CELL * 8 * cells
+    total = mg + guess + other
+    achieved = total / (res["ms"] / res["steps"] * 1e-3) / 1e9
+    return {"bytes_per_step": total, "multigrid_bytes_per_step": mg, "achieved": achieved, "unit": "GB/s",
+            "frac": achieved / peak}
+
+
+def vcycle_rooflines(V, torch, args, sim, peak):
+    """Whole FP64 V-cycles of the MAC and FEM systems of the bench grid, back
+    to back as mg_test.cc:36-43 times them, against their canonical bytes."""
+    m, n = (int(x) for x in args.grid.split("x"))
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(1)
+    for name, cls, mm, nn, c1, c2 in (("MAC", V.MgsMac, m, n, sim.dx, sim.dy),
+                                      ("FEM", V.MgsFem, m + 1, n + 1, sim.dx, sim.dy)):
+        s = cls(mm, nn, c1, c2)
+        s.b.copy_(torch.randn(mm * nn, dtype=torch.float64, device="cuda", generator=g))
+        ms, nbytes = s.profile(2, 50)
+        a = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms_per_vcycle": ms, "canonical_bytes": nbytes, "achieved": a, "frac": a / peak}
+        del s
+    return out
+
+
+def single_projection(V, torch, args, stream, peak):
+    """The single-projection workload: the MAC system on a 2048x1024 grid of
+    square cells (mgs_mac's operator), source the seeded zero-mean sum of 64
+    Gaussians, solved from zero to 1e-10 in each precision. Reports V-cycles,
+    CUDA-event time per solve and per V-cycle, canonical GB/s, and the
+    max-relative difference from an FP64 solve run on past its tolerance
+    (8 more V-cycles, where the iterates stop changing)."""
+    m, n = 2048, 1024
+    dx = 1. / m
+    b = torch.from_numpy(V.projection_source(m, n, seed=2048)).cuda()
+    s = V.MgsMac(m, n, dx, dx, stream=stream)
+    s.b.copy_(b)
+    s.z.zero_()
+    s.solve_v_cycle(rtol=1e-10, precision="fp64")
+    for _ in range(8):
+        s.v_cycle()
+    zt = s.z.clone()
+    ms64, by64 = s.profile(2, 20)
+    out = {"grid": f"{m}x{n}", "source": "zero-mean sum of 64 Gaussians, seed 2048", "rtol": 1e-10,
+           "ms_per_fp64_vcycle_mg_test": ms64}
+    cells = m * n
+    for prec in ("fp64", "mixed", "hybrid"):
+        for rep in range(2):     # the first solve of a precision builds its arrays
+            s.z.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            v, rel = s.solve_v_cycle(rtol=1e-10, precision=prec)
+            e1.record(stream)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        pts = by64 / (8 * (3. * 4 + 4.5))
+        if prec == "fp64":
+            per = by64
+        elif prec == "hybrid":
+            per = by64 / 2 + cells * (3. * 4 + 4.5) * 4
+        else:
+            per = by64 / 2 + 40. * cells
+        err = float((s.z - zt).abs().max() / zt.abs().max())
+        achieved = v * per / (ms * 1e-3) / 1e9
+        out[prec] = {"vcycles": v, "rel_res": rel, "ms_per_solve": ms, "ms_per_vcycle": ms / v,
+                     "canonical_bytes_per_vcycle": per, "achieved_gbs": achieved, "frac": achieved / peak,
+                     "max_rel_diff_vs_fp64_converged": err}
+    out["levels_points"] = pts
+    return out
 
 
 def e2e_run(V, torch, text, args, stream, steps, ws):
@@ -350,7 +442,8 @@ def main():
         clocks = ClockSampler(local) if name == "fast" or args.only else None
         f, dt, ms, vc, st, ck, solves = time_config(V, torch, text, args, prec, guess, stream, ws, clocks)
         results[name] = dict(ms=ms, vc=vc, clocks=ck, solves=solves, newton=st["newton_steps"],
-                             launches=st["kernel_launches"])
+                             launches=st["kernel_launches"], stats=st, steps=args.steps,
+                             vcycle_bytes=f.vcycle_bytes())
         if name == modes[-1][0]:
             keep = (f, dt)
         else:
@@ -393,6 +486,15 @@ def main():
         line["variants"] = variants
     f, dt = keep
     line["roofline"] = roofline(V, torch, args)
+    peak = line["roofline"]["peak"]
+    line["roofline"]["canonical"] = {
+        "note": "SURVEY-style canonical bytes (fusion-independent word counts per point) over CUDA-event time",
+        "step": canonical_step(f, head, peak),
+        "vcycle": vcycle_rooflines(V, torch, args, f, peak)}
+    if "plain" in results:
+        line["roofline"]["canonical"]["step_plain_fp64"] = canonical_step(f, results["plain"], peak)
+    if not args.only and ws == 1:
+        line["single_projection"] = single_projection(V, torch, args, stream, peak)
     if not args.no_e2e:
         e2e_steps = args.steps
         ms, bi, bo = e2e_run(V, torch, text, args, stream, e2e_steps, ws)

@@ -153,6 +153,38 @@ int vdi_sim_set_state(vdi_sim* sim, const vdi_state* h_state);
 int vdi_sim_get_tracers(vdi_sim* sim, double* h_xy, long count);
 int vdi_sim_set_tracers(vdi_sim* sim, const double* h_xy, long count);
 
+/* The simulation's parameters as they stand (vdi_sim_set_nif_mode changes
+ * the frame fields). */
+int vdi_sim_get_params(const vdi_sim* sim, vdi_params* out);
+/* fluid_2d::init_tracers (fluid_2d.cc:495-502) alone: places the tracers
+ * again with the process's rand(), as vdi_sim_init_fields does. */
+int vdi_sim_init_tracers(vdi_sim* sim);
+/* fluid_2d::update_tracers (fluid_2d.cc:507-526) alone: moves the tracers
+ * by dt with the bilinearly interpolated velocity of the current state. */
+int vdi_sim_update_tracers(vdi_sim* sim, double dt);
+/* fluid_2d::set_nif_mode(mode, w) (declared at fluid_2d.hh:75; the
+ * reference gives it no body): switches the non-inertial frame between off
+ * (0), the velocity at the centre (1, nif_center, fileinfo.cc:96-98) and the
+ * velocity averaged over the columns within w of the axis (2, nif_range w,
+ * fileinfo.cc:99-101, 179-191). A window without a column returns
+ * VDI_ERR_CONFIG ("Velocity window for non-inertial frame is too small").
+ * The next step is captured again. */
+int vdi_sim_set_nif_mode(vdi_sim* sim, int mode, double w);
+
+/* gas_layer::update(t, dt) (gas_layer.cc:38-48, with gas_layer_solve's
+ * calc_p_and_tau, gas_layer_solve.cc:188-249) alone, on the simulation's
+ * current liquid velocity: keeps the previous pressure and shear stress,
+ * advances the height, solves the gas pressure by Newton iteration and sets
+ * the liquid pressure and the shear stress with its boundary conditions.
+ * The simulation clock does not move (fluid_2d::step_forward moves it).
+ * Returns VDI_ERR_NEWTON_NOT_CONVERGED or VDI_ERR_TRI_SINGULAR where the
+ * reference calls fatal_error. */
+int vdi_gas_update(vdi_sim* sim, double dt);
+/* gas_layer_solve::init_fields (gas_layer_solve.cc:32-53) alone: the
+ * parabolic height, its time derivative -V, zero gas pressure and shear
+ * stress. */
+int vdi_gas_init_fields(vdi_sim* sim);
+
 /* Per-solver statistics since the last reset (the reference's
  * tgmg_predict::avg_iters and wall-clock counters, mgs_common.hh:47-55). */
 typedef struct vdi_stats {
@@ -169,8 +201,23 @@ int vdi_sim_stats(vdi_sim* sim, vdi_stats* out, int reset);
 
 /* Device pointers to the state arrays (read-only use by callers that keep
  * data on the device). which: 0 u, 1 v, 2 p, 3 gas h, 4 gas pg, 5 gas gp,
- * 6 the last MAC source, 7 the last MAC solution (m*n each). */
+ * 6 the last MAC source, 7 the last MAC solution (m*n each), 8 the last FEM
+ * source ((m+1)*(n+1)), the contents of fluid_2d::src after a step; the gas
+ * layer's 9 previous liquid pressure p_old (m+1), 10 shear stress tau and
+ * 11 its previous value tau_old (m+4 each, two ghosts per side), 12 ht and
+ * 13 fbd (m each). */
 int vdi_sim_device_field(vdi_sim* sim, int which, double** d_ptr, size_t* count);
+
+/* Measurement helper (no reference counterpart): the canonical algorithmic
+ * bytes of one solve-loop iteration of each of the simulation's multigrid
+ * systems (MAC, FEM, VX, VY; 0 for a system the simulation does not have),
+ * with the hierarchies as they stand, for the given vdi_mg_precision. A
+ * V-cycle moves (3 (nu1 + nu2) + 4.5) words per point of every level:
+ * 8-byte words in FP64, 4-byte words on FP32 levels (every level in
+ * VDI_MG_MIXED, the coarse levels in VDI_MG_HYBRID). VDI_MG_MIXED adds its
+ * FP64 refinement, 40 bytes per finest point (residual: z, b in, FP32 r
+ * out; update: z in and out, FP32 correction in). */
+int vdi_sim_vcycle_bytes(const vdi_sim* sim, int precision, double* out4);
 
 /* ----------------------------------------------------------- autotuning
  * Picks, by timing on this GPU with the simulation's own arrays, the launch
@@ -336,18 +383,23 @@ int vdi_unet_params(vdi_unet* net, float* h_buf, long count, int to_device);
  * out_scale * rms(residual) / xxsp, prolonged back, is added to the guess. */
 int vdi_sim_attach_unet(vdi_sim* sim, vdi_unet* net, int factor, double out_scale);
 
-/* vdi_mg_solve_noalloc has no counterpart in the reference. It is the FP64
- * solve of vdi_mg_create + vdi_mg_solve for callers that must not allocate
- * device memory, such as an application that owns every device allocation
- * itself or code running where an allocation would stall or fail. It
- * allocates nothing: besides the caller's d_b and d_z it uses one static
- * device array of about 5 MB that every GPU loading the library holds until
- * exit. Grids are limited to 262144 unknowns (m*n); larger ones return
- * VDI_ERR_UNSUPPORTED_SIZE. The first call on a device looks up the array's
- * device address and should come before any stream capture. Calls share the
- * array, so calls that overlap on the GPU (other streams or host threads)
- * race. Arguments are those of vdi_mg_create and vdi_mg_solve; stream may
- * be NULL. */
+/* vdi_mg_solve_noalloc has no counterpart in the reference. It is an FP64
+ * multigrid solve of the systems of vdi_mg_create + vdi_mg_solve for callers
+ * that must not allocate device memory, such as an application that owns
+ * every device allocation itself or code running where an allocation would
+ * stall or fail. It allocates nothing: besides the caller's d_b and d_z it
+ * uses one static device array of about 5 MB that every GPU loading the
+ * library holds until exit. Grids are limited to 262144 unknowns (m*n);
+ * larger ones return VDI_ERR_UNSUPPORTED_SIZE. Its coarsest level is
+ * smoothed rather than solved with a precomputed inverse, so its V-cycle
+ * count can differ from vdi_mg_solve's; it stops on the same residual test.
+ * The first call on a device looks up the array's device address and should
+ * come before any stream capture. Calls share the array: two calls that
+ * overlapped on the GPU would race on it. The entry point holds a
+ * process-wide lock for the whole call and returns only once its solve has
+ * finished, so calls from different host threads run one after another.
+ * Arguments are those of vdi_mg_create and vdi_mg_solve; stream may be
+ * NULL. */
 int vdi_mg_solve_noalloc(int kind, int m, int n, double c1, double c2, int x_sym, const double* d_b, double* d_z,
                          double rtol, int max_vcycles, void* stream, vdi_mg_result* res);
 

@@ -225,6 +225,41 @@ def mac_matrix(m, n, xxsp, yysp, neumann_bottom=False):
     return _assemble(m, n, diag, left, right, down, up)
 
 
+def mac_direct_solve(m, n, xxsp, yysp, b):
+    """Exact solve of mac_matrix(m, n, xxsp, yysp) z = b (mgs_mac.hh:33-48)
+    for large grids, by separation of variables. The operator is
+    T_x (x) I + I (x) T_y with T_x the cell-centred Neumann-Neumann second
+    difference, which the orthonormal DCT-II diagonalises (eigenvalues
+    -4 xxsp sin^2(pi k / 2m)), and T_y tridiagonal (Dirichlet ghost reflection
+    at the bottom, Neumann at the top). So: DCT-II along x, one tridiagonal
+    solve in y per mode (the Thomas algorithm, vectorised over the modes;
+    every system is symmetric negative definite), inverse DCT. Cost
+    O(m n log m); accuracy that of FP64 arithmetic on the conditioning of the
+    system, with no iteration to converge."""
+    import scipy.fft as sfft
+    B = np.asarray(b, dtype=np.float64).reshape(n, m)
+    Bh = sfft.dct(B, type=2, norm="ortho", axis=1)
+    mu = -4. * xxsp * np.sin(np.pi * np.arange(m) / (2. * m)) ** 2
+    d = np.empty((n, m))
+    d[:] = -2. * yysp
+    d[0] = -3. * yysp
+    d[n - 1] = -yysp if n > 1 else -3. * yysp
+    d += mu[None, :]
+    c = np.empty((n, m))
+    y = np.empty((n, m))
+    c[0] = yysp / d[0]
+    y[0] = Bh[0] / d[0]
+    for j in range(1, n):
+        den = d[j] - yysp * c[j - 1]
+        c[j] = yysp / den
+        y[j] = (Bh[j] - yysp * y[j - 1]) / den
+    Z = np.empty((n, m))
+    Z[n - 1] = y[n - 1]
+    for j in range(n - 2, -1, -1):
+        Z[j] = y[j] - c[j] * Z[j + 1]
+    return sfft.idct(Z, type=2, norm="ortho", axis=1).ravel()
+
+
 def fem_coeffs(dx, dy):
     """mgs_fem.cc:8-11: the bilinear finite-element stencil constants."""
     dydx, dxdy = dy / dx, dx / dy

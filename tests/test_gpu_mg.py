@@ -23,17 +23,8 @@ def _torch():
 def gaussians_rhs(m, n, seed, k=64):
     """Zero-mean sum of k Gaussians (centres uniform, widths 0.01-0.1 of the
     domain, amplitudes N(0,1)): the single-projection workload's RHS."""
-    rng = np.random.default_rng(seed)
-    x = (np.arange(m) + 0.5) / m
-    y = (np.arange(n) + 0.5) / n * (n / m)
-    X, Y = np.meshgrid(x, y)
-    b = np.zeros((n, m))
-    for _ in range(k):
-        cx, cy = rng.uniform(0, 1), rng.uniform(0, n / m)
-        w = rng.uniform(0.01, 0.1)
-        a = rng.standard_normal()
-        b += a * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * w * w))
-    return (b - b.mean()).ravel()
+    from vdropimpact_b200 import projection_source
+    return projection_source(m, n, seed, k)
 
 
 def _rel(a, b):

@@ -172,3 +172,15 @@ def test_newton_threshold_constants():
     """gas_layer_solve.hh:11-18."""
     assert vo.NEWTON_THRESH == (np.finfo(float).eps * 1e8) ** 2
     assert vo.MAX_NEWTON_STEPS == 256
+
+
+@pytest.mark.parametrize("m,n", [(64, 32), (128, 128), (96, 40)])
+def test_mac_direct_solve_matches_sparse_lu(m, n):
+    """The separable exact MAC solve (the yardstick of the full-size
+    single-projection test) equals a sparse LU solve of mac_matrix."""
+    rng = np.random.default_rng(m + n)
+    b = rng.standard_normal(m * n)
+    xxsp, yysp = float(m * m), 2.25 * m * m
+    A = vo.mac_matrix(m, n, xxsp, yysp)
+    z = vo.mac_direct_solve(m, n, xxsp, yysp, b)
+    assert _rel(z, vo.DirectSolver(A).solve(b)) < 1e-12

@@ -5,7 +5,9 @@ The allocation-free entry point serves callers that cannot allocate device
 memory (an application that owns every allocation, or code where an
 allocation would stall); it takes its scratch from one static device array.
 Each case makes two calls in a row, since the array keeps the previous
-call's contents."""
+call's contents; one test interleaves systems that share the array, and one
+checks that calls after the first leave the device's free memory
+unchanged."""
 import ctypes as C
 
 import numpy as np
@@ -97,3 +99,74 @@ def test_noalloc_rejects_oversized_grid(L):
                                 C.c_void_p(dz.data_ptr()), C.c_double(1e-10), 200, None, C.byref(r))
     assert st == _abi.VDI_ERR_UNSUPPORTED_SIZE
     assert b"exceeds the maximum" in L.vdi_last_error()
+
+
+@pytest.mark.parametrize("kind,m,n,c1,c2,x_sym", [
+    (0, 512, 512, 1. / 512, 1. / 512, 0),      # MAC at the 262144-unknown limit
+    (1, 513, 511, 1. / 512, 1. / 510, 0),      # FEM, 262143 nodes
+])
+def test_noalloc_near_the_size_limit(L, kind, m, n, c1, c2, x_sym):
+    """The coarsest level is smoothed here and solved exactly by the
+    allocating solve: both reach the residual tolerance and agree within the
+    tolerance the solves leave."""
+    for call, seed in enumerate((5, 6)):
+        b = _gauss(m, n, seed)
+        if kind == 1:
+            b = b.reshape(n, m)
+            b[0, :] = 50.0
+            b = b.ravel()
+        za, va = _solve_allocating(L, kind, m, n, c1, c2, x_sym, b)
+        zn, vn = _solve_noalloc(L, kind, m, n, c1, c2, x_sym, b)
+        scale = max(np.abs(za).max(), 1e-300)
+        assert np.abs(zn - za).max() / scale <= TOL, (kind, call)
+        assert abs(vn - va) <= 1, (kind, call, vn, va)
+
+
+def test_noalloc_interleaved_systems(L):
+    """MAC, FEM, viscous, MAC again: the hierarchies of all three carve the
+    same array, so each call must rely on nothing another call left there."""
+    cases = [(0, 256, 128, 1. / 256, 1. / 256, 0), (1, 257, 129, 1. / 256, 1. / 256, 0),
+             (3, 128, 64, 2.0, 2.0, 1), (0, 256, 128, 1. / 256, 1. / 256, 0)]
+    for k, (kind, m, n, c1, c2, x_sym) in enumerate(cases):
+        b = _gauss(m, n, 10 + k)
+        if kind == 1:
+            b = b.reshape(n, m)
+            b[0, :] = 50.0
+            b = b.ravel()
+        za, va = _solve_allocating(L, kind, m, n, c1, c2, x_sym, b)
+        zn, vn = _solve_noalloc(L, kind, m, n, c1, c2, x_sym, b)
+        assert np.abs(zn - za).max() / max(np.abs(za).max(), 1e-300) <= TOL, k
+        assert vn == va, (k, vn, va)
+
+
+def test_noalloc_leaves_free_device_memory_unchanged(L):
+    """After a first call of each kind (which looks up the array's address and
+    loads the kernels), further calls, of a cached system and of new ones
+    (new coefficients, a new grid), do not change the device's free memory,
+    and neither do more new systems than the entry point keeps."""
+    import torch
+    from vdropimpact_b200 import _abi
+    m, n = 256, 128
+    db = torch.from_numpy(_gauss(m, n, 20)).cuda()
+    dz = torch.zeros_like(db)
+    r = _abi.VdiMgResult()
+
+    def call(kind, mm, nn, c1, c2, x_sym):
+        dz.zero_()
+        torch.cuda.synchronize()
+        st = L.vdi_mg_solve_noalloc(kind, mm, nn, C.c_double(c1), C.c_double(c2), x_sym,
+                                    C.c_void_p(db.data_ptr()), C.c_void_p(dz.data_ptr()), C.c_double(1e-10), 200,
+                                    None, C.byref(r))
+        _abi.check(st, "vdi_mg_solve_noalloc")
+
+    for kind, c in ((0, 1. / 256), (2, 0.4), (3, 0.4)):
+        call(kind, m, n, c, c, 1 if kind else 0)
+    call(1, 129, 65, 1. / 128, 1. / 128, 0)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    call(0, m, n, 1. / 256, 1. / 256, 0)                 # cached
+    call(0, 128, 64, 1. / 128, 1. / 128, 0)              # new grid
+    for q in range(20):                                  # new coefficients, past the cache's bound
+        call(2, m, n, 0.4 + 0.01 * q, 0.4 + 0.01 * q, 1)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0

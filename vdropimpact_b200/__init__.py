@@ -24,7 +24,7 @@ from ._abi import (VDI_MG_FP64, VDI_MG_MIXED, VDI_GUESS_EXTRAPOLATE, VDI_GUESS_L
                    VDI_MG_FEM, VDI_MG_VISC_U, VDI_MG_VISC_V, VdiError, check, lib)
 
 __all__ = ["Fluid2D", "MgsMac", "MgsMacNeumann", "MgsFem", "ViscoImpl", "TriSolve", "VdiError", "params_from_cfg",
-           "VDI_MG_FP64", "VDI_MG_MIXED", "VDI_GUESS_EXTRAPOLATE", "VDI_GUESS_LEARNED"]
+           "VDI_MG_FP64", "VDI_MG_MIXED", "VDI_GUESS_EXTRAPOLATE", "VDI_GUESS_LEARNED", "projection_source"]
 
 _PREC = {"fp64": VDI_MG_FP64, "mixed": VDI_MG_MIXED, "hybrid": _abi.VDI_MG_HYBRID, VDI_MG_FP64: VDI_MG_FP64,
          VDI_MG_MIXED: VDI_MG_MIXED, _abi.VDI_MG_HYBRID: _abi.VDI_MG_HYBRID}
@@ -251,6 +251,14 @@ class Fluid2D:
         check(lib().vdi_sim_attach_unet(self._h, net._h, factor, float(net.out_scale)), "vdi_sim_attach_unet")
         self._unet = net
 
+    def vcycle_bytes(self, precision=None) -> dict:
+        """Canonical algorithmic bytes of one solve-loop iteration of each
+        multigrid system (measurement helper; see vdi_sim_vcycle_bytes)."""
+        out = (C.c_double * 4)()
+        prec = _PREC[precision if precision is not None else self.prm.mg_precision]
+        check(lib().vdi_sim_vcycle_bytes(self._h, prec, out), "vdi_sim_vcycle_bytes")
+        return dict(zip(("MAC", "FEM", "VX", "VY"), list(out)))
+
     def device_field(self, which: int):
         p = _abi._dp()
         n = C.c_size_t()
@@ -338,6 +346,26 @@ def sweep_configs(count: int, seed: int = 0, sizes=(256, 512, 1024)):
             "R 1.5e-3", f"V {V:.6g}", "gamma 1.4", "sigma 72e-3", "mug 1.820775e-5", "Pamb 1e5", "x_sym",
             "implicit_visc", "gas_layer_model"]) + "\n")
     return out
+
+
+def projection_source(m: int, n: int, seed: int, count: int = 64) -> np.ndarray:
+    """The source of the single-projection workload on an m x n cell grid of
+    a domain 1 wide and n/m high: the sum of `count` Gaussians (centres
+    uniform over the domain, widths uniform in 0.01-0.1 of its width,
+    amplitudes N(0,1), drawn from a generator seeded with `seed`), minus its
+    mean; float64, m*n values in the row order ij = i + m*j of mgs_mac."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(m) + 0.5) / m
+    y = (np.arange(n) + 0.5) / n * (n / m)
+    b = np.zeros((n, m))
+    for _ in range(count):
+        cx, cy = rng.uniform(0, 1), rng.uniform(0, n / m)
+        w = rng.uniform(0.01, 0.1)
+        a = rng.standard_normal()
+        gx = np.exp(-(x - cx) ** 2 / (2 * w * w))
+        gy = np.exp(-(y - cy) ** 2 / (2 * w * w))
+        b += a * np.outer(gy, gx)
+    return (b - b.mean()).ravel()
 
 
 def sweep_cost(cfg: str) -> float:

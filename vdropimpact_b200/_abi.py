@@ -121,6 +121,13 @@ _SIGS = [
     ("vdi_sim_set_tracers", C.c_int, [C.c_void_p, _dp, C.c_long]),
     ("vdi_sim_stats", C.c_int, [C.c_void_p, C.POINTER(VdiStats), C.c_int]),
     ("vdi_sim_device_field", C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(C.c_size_t)]),
+    ("vdi_sim_vcycle_bytes", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    ("vdi_sim_get_params", C.c_int, [C.c_void_p, C.POINTER(VdiParams)]),
+    ("vdi_sim_init_tracers", C.c_int, [C.c_void_p]),
+    ("vdi_sim_update_tracers", C.c_int, [C.c_void_p, C.c_double]),
+    ("vdi_sim_set_nif_mode", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("vdi_gas_update", C.c_int, [C.c_void_p, C.c_double]),
+    ("vdi_gas_init_fields", C.c_int, [C.c_void_p]),
     ("vdi_sim_autotune", C.c_int, [C.c_void_p, C.POINTER(VdiTune)]),
     ("vdi_sim_set_tuning", C.c_int, [C.c_void_p, C.POINTER(VdiTune)]),
     ("vdi_sim_profile", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float)]),

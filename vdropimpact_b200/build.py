@@ -23,11 +23,14 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
 # Stencil and gas-layer kernels follow the reference's expression order
 # exactly; FMA contraction would change their rounding.
 EXACT = {"step_kernels.cu", "gas.cu", "liftoff.cu"}
-SOURCES = ["mg.cu", "step_kernels.cu", "gas.cu", "liftoff.cu", "sim.cu", "unet.cu", "batch.cu", "host_api.cu"]
+SOURCES = ["mg.cu", "step_kernels.cu", "gas.cu", "liftoff.cu", "sim.cu", "unet.cu"]
 
 
 def _sources():
-    return [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    missing = [s for s in SOURCES if not os.path.exists(os.path.join(CSRC, s))]
+    if missing:
+        raise FileNotFoundError(f"CUDA sources missing from {CSRC}: {missing}")
+    return list(SOURCES)
 
 
 def _deps():

@@ -156,26 +156,23 @@ __device__ int tri_solve_block(int n, int Np, double* a, double* b, double* c, d
     return info_s;
 }
 
-__global__ void k_tri_solve(int n, int Np, double* ga, double* gb, double* gc, double* gd, int* out_pivoted,
-                            int use_smem) {
+/** One CTA solves the whole system in shared memory (launch_tri_solve
+ * rejects systems that do not fit). */
+__global__ void k_tri_solve(int n, int Np, double* ga, double* gb, double* gc, double* gd, int* out_pivoted) {
     extern __shared__ __align__(16) double sm[];
     __shared__ double ws[33];
-    double *a, *b, *c, *d, *x;
-    if (use_smem) {
-        a = sm; b = a + Np; c = b + Np; d = c + Np; x = d + Np;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            a[i] = ga[i]; b[i] = gb[i]; c[i] = gc[i]; d[i] = gd[i];
-        }
-        __syncthreads();
-    } else {
-        // global scratch lives after the four arrays in ga's allocation
-        a = ga; b = gb; c = gc; d = gd; x = nullptr;
+    double* a = sm;
+    double* b = a + Np;
+    double* c = b + Np;
+    double* d = c + Np;
+    double* x = d + Np;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a[i] = ga[i]; b[i] = gb[i]; c[i] = gc[i]; d[i] = gd[i];
     }
-    (void)ws;
+    __syncthreads();
     int piv = 0;
     int info = tri_solve_block(n, Np, a, b, c, d, x, ws, &piv);
-    if (use_smem)
-        for (int i = threadIdx.x; i < n; i += blockDim.x) gd[i] = d[i];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) gd[i] = d[i];
     if (threadIdx.x == 0 && out_pivoted) out_pivoted[0] = info != 0 ? -info : piv;
 }
 
@@ -461,7 +458,7 @@ int launch_tri_solve(cudaStream_t s, int n, double* a, double* b, double* c, dou
                                       int(gas_smem_limit())));
         attr_set = true;
     }
-    k_tri_solve<<<1, GAS_THREADS, bytes, s>>>(n, Np, a, b, c, d, d_pivoted, 1);
+    k_tri_solve<<<1, GAS_THREADS, bytes, s>>>(n, Np, a, b, c, d, d_pivoted);
     VDI_CUDA(cudaGetLastError());
     return VDI_OK;
 }

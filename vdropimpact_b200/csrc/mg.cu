@@ -32,6 +32,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 namespace vdi {
 
@@ -1996,6 +1997,19 @@ int mg_kernels_per_iteration(const MG* mg, int precision) {
     return k;
 }
 
+double mg_vcycle_bytes(const MG* mg, int fine_word, int coarse_word) {
+    // canonical bytes of a V-cycle: per level, each smoothing sweep reads z
+    // and b and writes z, and the transfers move 4.5 words per point
+    const double per = 3. * (mg->nu1 + mg->nu2) + 4.5;
+    double fine = 0, coarse = 0;
+    if (mg->general) {
+        for (int q = 0; q < mg->gen.nlev(); q++) (q ? coarse : fine) += double(mg->gen.size(q));
+    } else {
+        for (int q = 0; q < mg->nlev; q++) (q ? coarse : fine) += double(mg->size(q));
+    }
+    return per * (fine * fine_word + coarse * coarse_word);
+}
+
 int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, double* z, float* ms, double* bytes) {
     if (iters < 1 || which < 0 || which > 3) return VDI_ERR_INVALID_ARGUMENT;
     if (which >= 2) {
@@ -2023,14 +2037,7 @@ int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, do
         cudaEventDestroy(e1);
         VDI_TRY(st);
         *ms = t / iters;
-        // canonical bytes of a V-cycle: per level, each smoothing sweep reads
-        // z and b and writes z, and the transfers move 4.5 words per point
-        double pts = 0;
-        if (mg->general)
-            for (int q = 0; q < mg->gen.nlev(); q++) pts += double(mg->gen.size(q));
-        else
-            for (int q = 0; q < mg->nlev; q++) pts += double(mg->size(q));
-        *bytes = which == 2 ? (3. * (mg->nu1 + mg->nu2) + 4.5) * 8 * pts : 0.;
+        *bytes = which == 2 ? mg_vcycle_bytes(mg, 8, 8) : 0.;
         return VDI_OK;
     }
     if (mg->nmulti64 < 1) return VDI_ERR_INVALID_ARGUMENT;
@@ -2091,12 +2098,16 @@ int mg_apply(MG* mg, cudaStream_t s, const double* z, double* y) {
 }  // namespace vdi
 
 // ======================================================= allocation-free solve
-// vdi_mg_solve_noalloc: the same FP64 multigrid solve as vdi_mg_create +
-// vdi_mg_solve, for callers that must not allocate device memory: an
-// application that owns every device allocation itself (a fixed memory
-// budget or its own pool), or code that runs where an allocation would
-// stall or fail (a real-time loop). Every device buffer the solve needs
-// beyond the caller's b and z comes from one file-scope __device__ array.
+// vdi_mg_solve_noalloc: an FP64 multigrid solve of the same systems as
+// vdi_mg_create + vdi_mg_solve, for callers that must not allocate device
+// memory: an application that owns every device allocation itself (a fixed
+// memory budget or its own pool), or code that runs where an allocation
+// would stall or fail (a real-time loop). Every device buffer the solve
+// needs beyond the caller's b and z comes from one file-scope __device__
+// array. Its hierarchy differs from the allocating one in one respect: the
+// coarsest level is smoothed, not solved with a precomputed inverse (which
+// would need an allocation), and the MAC cluster coarse cycle is not used;
+// solves still stop on the same FP64 residual test.
 
 namespace vdi {
 
@@ -2129,9 +2140,31 @@ struct NoallocEntry {
     MG* mg;
 };
 
+/** Hierarchies kept, least recently used first. A caller whose
+ * coefficients change every call (viscous systems whose vfx, vfy follow the
+ * timestep) would otherwise grow the list without bound. */
+static constexpr size_t NOALLOC_CACHE_MAX = 16;
+
 std::vector<NoallocEntry>& noalloc_cache() {
     static std::vector<NoallocEntry> c;
     return c;
+}
+
+/** Held for a whole call: the cache, the per-device base addresses and the
+ * scratch array are shared by every host thread. */
+std::mutex& noalloc_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+
+/** Deletes a hierarchy whose buffers were carved from the scratch array:
+ * the pointers are cleared first, so its destructor frees nothing. */
+void noalloc_drop(MG* g) {
+    g->z64.clear(); g->b64.clear(); g->t64.clear();
+    g->ctl = nullptr;
+    g->rd.partials = nullptr;
+    g->rd.counter = nullptr;
+    delete g;
 }
 
 /** Device address of g_noalloc_scratch on the current device, looked up once
@@ -2188,18 +2221,10 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
             g->b64[l] = reinterpret_cast<double*>(take(s));
         }
     }
-    auto forget = [&]() {
-        // the buffers belong to the static array: nothing to free
-        g->z64.clear(); g->b64.clear(); g->t64.clear();
-        g->ctl = nullptr;
-        g->rd.partials = nullptr;
-        g->rd.counter = nullptr;
-    };
     if (!fits) {
         set_error("vdi_mg_solve_noalloc: %dx%d needs %zu bytes of scratch, more than the %zu available", k.m, k.n,
                   off, NOALLOC_SCRATCH_BYTES);
-        forget();
-        delete g;
+        noalloc_drop(g);
         return VDI_ERR_UNSUPPORTED_SIZE;
     }
     // shared-memory limits of the kernels this solve launches
@@ -2212,8 +2237,7 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
     if (e == cudaSuccess) e = fem_tile_attr<double>();
     if (e != cudaSuccess) {
         set_error("vdi_mg_solve_noalloc: %s", cudaGetErrorString(e));
-        forget();
-        delete g;
+        noalloc_drop(g);
         return VDI_ERR_CUDA;
     }
     *out = g;
@@ -2235,6 +2259,7 @@ extern "C" int vdi_mg_solve_noalloc(int kind, int m, int n, double c1, double c2
                   NOALLOC_MAX_UNKNOWNS);
         return VDI_ERR_UNSUPPORTED_SIZE;
     }
+    std::lock_guard<std::mutex> lock(noalloc_mutex());
     int dev = 0;
     VDI_CUDA(cudaGetDevice(&dev));
     unsigned char* base = nullptr;
@@ -2245,12 +2270,24 @@ extern "C" int vdi_mg_solve_noalloc(int kind, int m, int n, double c1, double c2
         key.c1 = 1. / (c1 * c1);
         key.c2 = 1. / (c2 * c2);
     }
+    auto& cache = noalloc_cache();
     MG* g = nullptr;
-    for (auto& e : noalloc_cache())
-        if (e.key == key) g = e.mg;
+    for (size_t q = 0; q < cache.size(); q++) {
+        if (cache[q].key == key) {
+            NoallocEntry hit = cache[q];      // most recently used goes last
+            cache.erase(cache.begin() + q);
+            cache.push_back(hit);
+            g = hit.mg;
+            break;
+        }
+    }
     if (!g) {
         VDI_TRY(noalloc_build(key, base, &g));
-        noalloc_cache().push_back(NoallocEntry{key, g});
+        if (cache.size() >= NOALLOC_CACHE_MAX) {
+            noalloc_drop(cache.front().mg);
+            cache.erase(cache.begin());
+        }
+        cache.push_back(NoallocEntry{key, g});
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // the array keeps the previous call's contents: restart the control

@@ -53,6 +53,7 @@ struct vdi_sim {
     double* d_vframe = nullptr;
     double* d_tm = nullptr;     // tracer positions x0, y0, x1, ... (2 * ntrace)
     double* d_vacc = nullptr;   // the non-inertial frame's velocity of a step
+    double* d_time_aside = nullptr;   // clock for a gas-layer update run alone
     int* d_err = nullptr;
     GasStats* d_gstats = nullptr;
     MG* mg[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -262,6 +263,27 @@ int capture_step(vdi_sim* S, double dt) {
     return VDI_OK;
 }
 
+/** fileinfo.cc:179-191: the columns whose centres lie within nif_r of the
+ * axis (from the axis when x_sym), for nif_range. */
+int nif_window(vdi_params* P, double nif_r) {
+    const int m = P->m;
+    const double xsp = 1. / ((P->bx - P->ax) / m);
+    int b = int((nif_r - P->ax) * xsp + 0.5), a;
+    if (b >= m) b = m - 1;
+    if (P->x_sym) a = 0;
+    else {
+        a = int((-nif_r - P->ax) * xsp + 0.5);
+        if (a < 0) a = 0;
+    }
+    if (b - a <= 0) {
+        set_error("Velocity window for non-inertial frame is too small");
+        return VDI_ERR_CONFIG;
+    }
+    P->nif_a = a;
+    P->nif_b = b;
+    return VDI_OK;
+}
+
 int parse_cfg(const char* text, vdi_params* P) {
     // fileinfo.cc:11-193 for the gas_layer_model path
     int m = -1, n = -1, nframes = -1, glo = 0;
@@ -348,23 +370,7 @@ int parse_cfg(const char* text, vdi_params* P) {
     if (ntrace < 0) { set_error("Value of tracers invalid"); return VDI_ERR_CONFIG; }
     P->ntrace = ntrace;
     P->nif_mode = nif_mode;
-    if (nif_mode == 2) {
-        // fileinfo.cc:179-191: the columns whose centres lie within nif_r
-        const double xsp = 1. / ((P->bx - P->ax) / m);
-        int b = int((nif_r - P->ax) * xsp + 0.5), a;
-        if (b >= m) b = m - 1;
-        if (x_sym) a = 0;
-        else {
-            a = int((-nif_r - P->ax) * xsp + 0.5);
-            if (a < 0) a = 0;
-        }
-        if (b - a <= 0) {
-            set_error("Velocity window for non-inertial frame is too small");
-            return VDI_ERR_CONFIG;
-        }
-        P->nif_a = a;
-        P->nif_b = b;
-    }
+    if (nif_mode == 2) VDI_TRY(nif_window(P, nif_r));
     return VDI_OK;
 }
 
@@ -539,7 +545,8 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     S->d_vframe = misc + 1;
     S->hist = reinterpret_cast<GuessHist*>(misc + 2);
     if (P.ntrace > 0 && (st = alloc_zero(S, &S->d_tm, 2 * size_t(P.ntrace))) != VDI_OK) return fail(st);
-    if (P.nif_mode != 0 && (st = alloc_zero(S, &S->d_vacc, 1)) != VDI_OK) return fail(st);
+    if ((st = alloc_zero(S, &S->d_vacc, 1)) != VDI_OK) return fail(st);
+    if ((st = alloc_zero(S, &S->d_time_aside, 1)) != VDI_OK) return fail(st);
     double* ebuf;
     if ((st = alloc_zero(S, &ebuf, 1 + sizeof(GasStats) / 8 + 1)) != VDI_OK) return fail(st);
     S->d_err = reinterpret_cast<int*>(ebuf);
@@ -622,6 +629,20 @@ int vdi_sim_destroy(vdi_sim* S) {
     return VDI_OK;
 }
 
+/** fluid_2d::init_tracers (fluid_2d.cc:495-502): positions from the
+ * process's rand(), uniform over the domain. */
+static int place_tracers(vdi_sim* S) {
+    const vdi_params& P = S->prm;
+    std::vector<double> tm(2 * size_t(P.ntrace));
+    for (size_t k = 0; k < tm.size(); k += 2) {
+        tm[k] = P.ax + (P.bx - P.ax) / RAND_MAX * static_cast<double>(rand());
+        tm[k + 1] = P.ay + (P.by - P.ay) / RAND_MAX * static_cast<double>(rand());
+    }
+    VDI_CUDA(cudaMemcpyAsync(S->d_tm, tm.data(), tm.size() * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    return VDI_OK;
+}
+
 /** Restarts the lift-off search with the current state as state 0. */
 static int liftoff_restart(vdi_sim* S) {
     VDI_TRY(liftoff_reset_async(S->s, S->d_lift));
@@ -657,18 +678,59 @@ int vdi_sim_init_fields(vdi_sim* S) {
     VDI_TRY(launch_inviscid_bc(s, S->g, S->f, S->gas, 0.));
     VDI_TRY(launch_viscous_bc(s, S->g, S->f, S->gas));
     VDI_TRY(liftoff_restart(S));
-    if (S->prm.ntrace > 0) {
-        // fluid_2d::init_tracers (fluid_2d.cc:495-502): the process's rand()
-        const vdi_params& P = S->prm;
-        std::vector<double> tm(2 * size_t(P.ntrace));
-        for (size_t k = 0; k < tm.size(); k += 2) {
-            tm[k] = P.ax + (P.bx - P.ax) / RAND_MAX * static_cast<double>(rand());
-            tm[k + 1] = P.ay + (P.by - P.ay) / RAND_MAX * static_cast<double>(rand());
-        }
-        VDI_CUDA(cudaMemcpyAsync(S->d_tm, tm.data(), tm.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        VDI_CUDA(cudaStreamSynchronize(s));
-    }
+    if (S->prm.ntrace > 0) VDI_TRY(place_tracers(S));   // fluid_2d_sio.cc:30
     VDI_CUDA(cudaStreamSynchronize(s));
+    return VDI_OK;
+}
+
+int vdi_sim_get_params(const vdi_sim* S, vdi_params* out) {
+    if (!S || !out) return VDI_ERR_INVALID_ARGUMENT;
+    *out = S->prm;
+    return VDI_OK;
+}
+
+int vdi_sim_init_tracers(vdi_sim* S) {
+    if (!S) return VDI_ERR_INVALID_ARGUMENT;
+    if (S->prm.ntrace == 0) return VDI_OK;
+    return place_tracers(S);
+}
+
+int vdi_sim_update_tracers(vdi_sim* S, double dt) {
+    if (!S || !std::isfinite(dt)) return VDI_ERR_INVALID_ARGUMENT;
+    if (S->prm.ntrace == 0) return VDI_OK;
+    VDI_TRY(launch_tracers(S->s, S->g, S->f, S->d_tm, S->prm.ntrace, dt));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    return VDI_OK;
+}
+
+int vdi_sim_set_nif_mode(vdi_sim* S, int mode, double w) {
+    if (!S || mode < 0 || mode > 2) return VDI_ERR_INVALID_ARGUMENT;
+    vdi_params P = S->prm;
+    P.nif_mode = mode;
+    if (mode == 2) VDI_TRY(nif_window(&P, w));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
+    S->prm.nif_mode = P.nif_mode;
+    S->prm.nif_a = P.nif_a;
+    S->prm.nif_b = P.nif_b;
+    destroy_graph(S);   // the captured step holds the previous mode
+    return VDI_OK;
+}
+
+int vdi_gas_update(vdi_sim* S, double dt) {
+    if (!S || !(dt > 0)) return VDI_ERR_INVALID_ARGUMENT;
+    // the kernel advances the clock it is given by dt/2 (the step's
+    // half-time); run alone, it gets a copy so the simulation's clock stays
+    VDI_CUDA(cudaMemcpyAsync(S->d_time_aside, S->d_time, sizeof(double), cudaMemcpyDeviceToDevice, S->s));
+    VDI_TRY(launch_gas_update(S->s, S->gp, S->gas, S->f.u, S->f.v, S->prm.m + 4, S->d_vframe, dt,
+                              S->d_time_aside, S->gas_work, S->d_err, S->d_gstats));
+    return check_errors(S);
+}
+
+int vdi_gas_init_fields(vdi_sim* S) {
+    if (!S) return VDI_ERR_INVALID_ARGUMENT;
+    VDI_CUDA(cudaMemsetAsync(S->gas.tau, 0, (S->prm.m + 4) * 8, S->s));
+    VDI_TRY(launch_gas_init(S->s, S->gp, S->gas, S->prm.h0, S->prm.V));
+    VDI_CUDA(cudaStreamSynchronize(S->s));
     return VDI_OK;
 }
 
@@ -895,7 +957,28 @@ int vdi_sim_device_field(vdi_sim* S, int which, double** d_ptr, size_t* count) {
         case 5: *d_ptr = S->gas.gp; if (count) *count = m + 1; break;
         case 6: *d_ptr = S->src_mac; if (count) *count = size_t(m) * S->prm.n; break;
         case 7: *d_ptr = S->q; if (count) *count = size_t(m) * S->prm.n; break;
+        case 8: *d_ptr = S->src_fem; if (count) *count = size_t(m + 1) * (S->prm.n + 1); break;
+        case 9: *d_ptr = S->gas.gp_old; if (count) *count = m + 1; break;
+        case 10: *d_ptr = S->gas.tau; if (count) *count = m + 4; break;
+        case 11: *d_ptr = S->gas.tau_old; if (count) *count = m + 4; break;
+        case 12: *d_ptr = S->gas.ht; if (count) *count = m; break;
+        case 13: *d_ptr = S->gas.fbd; if (count) *count = m; break;
         default: return VDI_ERR_INVALID_ARGUMENT;
+    }
+    return VDI_OK;
+}
+
+int vdi_sim_vcycle_bytes(const vdi_sim* S, int precision, double* out4) {
+    if (!S || !out4) return VDI_ERR_INVALID_ARGUMENT;
+    if (precision != VDI_MG_FP64 && precision != VDI_MG_MIXED && precision != VDI_MG_HYBRID)
+        return VDI_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 4; k++) {
+        out4[k] = 0;
+        const MG* g = S->mg[k];
+        if (!g) continue;
+        if (precision == VDI_MG_FP64) out4[k] = mg_vcycle_bytes(g, 8, 8);
+        else if (precision == VDI_MG_HYBRID) out4[k] = mg_vcycle_bytes(g, 8, 4);
+        else out4[k] = mg_vcycle_bytes(g, 4, 4) + 40. * mg_fine_size(g);
     }
     return VDI_OK;
 }

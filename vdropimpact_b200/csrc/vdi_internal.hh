@@ -128,6 +128,11 @@ int mg_kernels_per_iteration(const MG* mg, int precision);
 int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, double* z, float* ms,
                double* bytes);
 
+/** Canonical algorithmic bytes of one V-cycle: (3 (nu1 + nu2) + 4.5) words
+ * per point of every level, the finest level's words fine_word bytes and the
+ * coarser levels' coarse_word bytes. */
+double mg_vcycle_bytes(const MG* mg, int fine_word, int coarse_word);
+
 /** r = b - A z on the finest level and ||r||_2 into *d_norm, on the stream
  * without host synchronisation (graph-capturable). */
 int mg_residual_async(MG* mg, cudaStream_t s, const double* b, const double* z, double* r, double* d_norm);

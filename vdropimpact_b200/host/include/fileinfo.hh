@@ -16,7 +16,7 @@ struct fileinfo {
         int ntrace;
         int nframes;
         int restart_freq;
-        /** The non-inertial frame mode; always 0 (outside the GPU path). */
+        /** The non-inertial frame mode: 0 off, 1 nif_center, 2 nif_range. */
         int nif_mode;
         bool implicit_visc;
         bool x_sym;
@@ -38,6 +38,10 @@ struct fileinfo {
         /** The output directory (the .cfg name with .odr). */
         char* filename;
         gas_layer* gl;
+        /** The columns [anif, bnif) whose velocity nif_range averages
+         * (fileinfo.hh:84-86, fileinfo.cc:179-191). */
+        int anif;
+        int bnif;
         fileinfo(const char* infile);
         ~fileinfo();
         /** The parameters in the C-ABI form. */

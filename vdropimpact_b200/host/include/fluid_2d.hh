@@ -5,9 +5,9 @@
 // (write_files and the Gnuplot formats of fluid_2d_sio.cc:140-224) and the
 // restart files (fluid_2d_sio.cc:39-119) are byte-compatible with the
 // reference's. fbase/fm hold host copies of u, v, p that sync_fields()
-// refreshes; the output and restart routines call it themselves. Tracers and
-// the non-inertial frame are outside the GPU path: a configuration that asks
-// for them stops with a fatal error.
+// refreshes; the output and restart routines call it themselves. Tracers
+// (tm, trace.N files and their restart block) and the non-inertial frame
+// run on the device with the rest of the step.
 #ifndef VDI_HOST_FLUID_2D_HH
 #define VDI_HOST_FLUID_2D_HH
 
@@ -38,9 +38,15 @@ class fluid_2d : public fileinfo {
         /** Tracer positions x0, y0, x1, ... (2*ntrace; host copy of the
          * device's, refreshed by sync_fields). */
         double* const tm;
-        /** A host source array of the node grid (me*ne), the right-hand side
-         * that a standalone visco_impl bound to this object solves with. */
+        /** The host source array of the node grid (me*ne), shared as in the
+         * reference (fluid_2d.cc:18-21): the right-hand side of problem
+         * objects bound to this fluid_2d. sync_fields() fills it with the
+         * device's last FEM source, which is what the reference's shared
+         * array holds after a step. */
         double* const src;
+        /** src + mn (fluid_2d.cc:18): in the reference the bottom-row terms of
+         * the MAC source, which the FEM source then overwrites. */
+        double* const s_bc;
         double time;
         int f_num;
         fluid_2d(const char* infile);
@@ -55,6 +61,16 @@ class fluid_2d : public fileinfo {
         void output(const char* prefix, const int mode, int sn, bool ghost = false);
         void output_pbase_full(int sn);
         void output_tracers(int sn);
+        /** fluid_2d::init_tracers (fluid_2d.cc:495-502) on the device tracers,
+         * then refreshes tm. */
+        void init_tracers();
+        /** fluid_2d::update_tracers (fluid_2d.cc:507-526): moves the device
+         * tracers by dt with the device velocity, then refreshes tm. */
+        void update_tracers(double dt);
+        /** Switches the non-inertial frame (fluid_2d.hh:75): mode 0 off, 1 the
+         * velocity at the centre, 2 averaged over the columns within w of the
+         * axis. The reference declares it without a body. */
+        void set_nif_mode(int mode, double w = 0);
         inline int timestep_select(double interval, double& adt) {
             int l = static_cast<int>(interval / dt_reg) + 1;
             adt = interval / l;

@@ -11,6 +11,11 @@ struct mgs_common {
     const int n;
     const int mn;
     int scount;
+    /** The TGMG problem-class flags (mgs_common.hh:19-26): no periodic
+     * direction, the default Gauss-Seidel mode. */
+    static const bool x_prd = false;
+    static const bool y_prd = false;
+    static const char gs_mode = 0;
     double t_prev;
     double t0;
     double* const z_prev;

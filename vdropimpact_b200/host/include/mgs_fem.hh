@@ -7,11 +7,41 @@
 #include "mgs_common.hh"
 #include "tgmg.hh"
 
+class fluid_2d;
+
 struct mgs_fem : public mgs_common {
-    const double dydx, dxdy, fm;
+    /** Spacing ratios and the bilinear element's stencil terms
+     * (mgs_fem.cc:8-11): centre fm (and its reciprocal), vertical fey, hey,
+     * horizontal fex, hex (the h* halves for edge nodes), corner fc. */
+    const double dydx, dxdy, fm, fm_inv, fey, hey, fex, hex, fc;
     double acc;
+    /** Bound to a simulation (mgs_fem.cc:8-18): its spacings on the node
+     * grid, and its src array as the source. */
+    mgs_fem(fluid_2d& f);
     /** The test constructor (mgs_fem.cc:26-30). */
     mgs_fem(int m_, int n_, double dx, double dy, double* b);
+    // The TGMG problem-class stencil (mgs_fem.hh:42-57), on the host arrays:
+    // the 9-point bilinear finite-element operator on m x n nodes. Nodes on
+    // the left, right and top edges carry half the element weight; the bottom
+    // row is a Dirichlet row with only its diagonal.
+    inline bool bottom(int ij) { return ij < m; }
+    inline double a_dl(int i, int ij) { return !bottom(ij) && i > 0 ? fc : 0; }
+    inline double a_dr(int i, int ij) { return !bottom(ij) && i < m - 1 ? fc : 0; }
+    inline double a_ul(int i, int ij) { return !bottom(ij) && below_top(ij) && i > 0 ? fc : 0; }
+    inline double a_ur(int i, int ij) { return !bottom(ij) && below_top(ij) && i < m - 1 ? fc : 0; }
+    inline double a_dc(int i, int ij) { return !bottom(ij) ? (inner_column(i) ? fey : hey) : 0; }
+    inline double a_uc(int i, int ij) { return !bottom(ij) && below_top(ij) ? (inner_column(i) ? fey : hey) : 0; }
+    inline double a_cl(int i, int ij) { return !bottom(ij) && i > 0 ? (below_top(ij) ? fex : hex) : 0; }
+    inline double a_cr(int i, int ij) { return !bottom(ij) && i < m - 1 ? (below_top(ij) ? fex : hex) : 0; }
+    inline double a_cc(int i, int ij) {
+        return (inner_column(i) ? 1 : 0.5) * (inner_row(ij) ? 1 : 0.5) * fm;
+    }
+    inline double inv_cc(int i, int ij, double v) {
+        return (inner_column(i) ? 1 : 2) * (inner_row(ij) ? 1 : 2) * fm_inv * v;
+    }
+    /** The off-diagonal part of A z at (i, ij); 0 on the Dirichlet bottom
+     * row (mgs_fem.cc:32-53). */
+    double mul_a(int i, int ij);
     inline void solve_v_cycle(double t) {
         initial_guess(t);
         solve_v_cycle();
@@ -25,6 +55,9 @@ struct mgs_fem : public mgs_common {
     tgmg<mgs_fem, double, double> mg;
     private:
         double dx_, dy_;
+        inline bool inner_column(int i) const { return i > 0 && i < m - 1; }
+        inline bool below_top(int ij) const { return ij < mn - m; }
+        inline bool inner_row(int ij) const { return ij >= m && ij < mn - m; }
 };
 
 #endif

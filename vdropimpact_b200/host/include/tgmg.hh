@@ -11,6 +11,12 @@
 #include "tgmg_predict.hh"
 #include "vdi.h"
 
+/** The absolute accuracy scale of tgmg_accuracy(scale, fac), the value the
+ * problem classes keep in their acc member (mgs_mac.cc:11, mgs_fem.cc:14,
+ * visco_impl.cc:12): scale * fac * machine epsilon. The device solves stop on
+ * the relative residual instead (rtol above). */
+inline double tgmg_accuracy(double scale, double fac) { return scale * fac * 2.220446049250313e-16; }
+
 /** The non-template part: device arrays and the C-ABI calls. */
 class vdi_tgmg_core {
     public:

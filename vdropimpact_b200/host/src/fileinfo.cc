@@ -39,6 +39,8 @@ fileinfo::fileinfo(const char* infile)
     fflags = ro.fflags;
     ntrace = params.ntrace;
     nif_mode = params.nif_mode;
+    anif = params.nif_a;
+    bnif = params.nif_b;
     nframes = params.nframes;
     restart_freq = ro.restart_freq;
     implicit_visc = params.implicit_visc != 0;

@@ -8,14 +8,37 @@
 #include <sys/stat.h>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 fluid_2d::fluid_2d(const char* infile)
     : fileinfo(infile), mn(m * n), me(m + 1), ne(n + 1), ml(m + 4), dx((bx - ax) / m), dy((by - ay) / n),
       xsp(1. / dx), ysp(1. / dy), xxsp(xsp * xsp), yysp(ysp * ysp),
       dt_reg(implicit_visc ? dx * tmult : dx * dx * rho * muinv * tmult * 0.25),
       fbase(new field[ml * (n + 4)]()), fm(fbase + 2 * ml + 2), tm(new double[2 * ntrace + 2]()), src(new double[me * ne]()),
-      time(0.), f_num(0), S(NULL), buf(new float[m > 123 ? m + 5 : 128]) {
+      s_bc(src + mn), time(0.), f_num(0), S(NULL), buf(new float[m > 123 ? m + 5 : 128]) {
     vdi_check(vdi_sim_create(&params, NULL, &S), "vdi_sim_create");
     vdi_check(vdi_sim_use_graph(S, 1), "vdi_sim_use_graph");
+    gl->attach(S);
+    gl->set_field_pointer(fm);
+}
+
+void fluid_2d::init_tracers() {
+    vdi_check(vdi_sim_init_tracers(S), "vdi_sim_init_tracers");
+    vdi_check(vdi_sim_get_tracers(S, tm, 2L * ntrace), "vdi_sim_get_tracers");
+}
+
+void fluid_2d::update_tracers(double dt) {
+    vdi_check(vdi_sim_update_tracers(S, dt), "vdi_sim_update_tracers");
+    vdi_check(vdi_sim_get_tracers(S, tm, 2L * ntrace), "vdi_sim_get_tracers");
+}
+
+void fluid_2d::set_nif_mode(int mode, double w) {
+    vdi_check(vdi_sim_set_nif_mode(S, mode, w), "vdi_sim_set_nif_mode");
+    vdi_params p;
+    vdi_check(vdi_sim_get_params(S, &p), "vdi_sim_get_params");
+    nif_mode = p.nif_mode;
+    anif = p.nif_a;
+    bnif = p.nif_b;
 }
 
 fluid_2d::~fluid_2d() {
@@ -104,6 +127,11 @@ void fluid_2d::sync_fields() {
     memcpy(g->tau, tau.data(), ml * sizeof(double));
     g->Vframe = s.Vframe;
     time = s.time;
+    double* d_src = NULL;
+    size_t count = 0;
+    vdi_check(vdi_sim_device_field(S, 8, &d_src, &count), "vdi_sim_device_field");
+    cudaError_t e = cudaMemcpy(src, d_src, count * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) fatal_error(cudaGetErrorString(e), 1);
 }
 
 void fluid_2d::push_fields() {

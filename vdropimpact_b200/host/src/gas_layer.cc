@@ -5,11 +5,20 @@
 
 #include <cstring>
 
+#include <cuda_runtime.h>
+
 #include "common.hh"
 
 gas_layer::gas_layer(int m_, double ax_, double bx_, double Vframe_)
     : m(m_), me(m_ + 1), ml(m_ + 4), ax(ax_), bx(bx_), dx((bx_ - ax_) / m_), Vframe(Vframe_), p(new double[me]()),
-      tau(new double[ml]()), p_old(new double[me]()), tau_old(new double[ml]()) {}
+      tau(new double[ml]()), p_old(new double[me]()), tau_old(new double[ml]()), sim_(NULL) {}
+
+void gas_layer::update(double t, double dt) {
+    if (sim_ == NULL) fatal_error("gas_layer::update: the gas layer belongs to no simulation", 1);
+    // the device keeps p_old and tau_old, computes the new fields and applies
+    // the shear-stress boundary conditions in one pass
+    calc_p_and_tau(t, dt);
+}
 
 gas_layer::~gas_layer() {
     delete[] tau_old;
@@ -37,7 +46,34 @@ void gas_layer::save_restart(FILE* outf) {
 
 gas_layer_solve::gas_layer_solve(int m_, double ax_, double bx_, double R_, double V_, double h0_)
     : gas_layer(m_, ax_, bx_, V_), R(R_), V(V_), h0(h0_), h(new double[m_]()), ht(new double[m_]()),
-      fbd(new double[m_]()), pg(new double[m_ + 1]()) {}
+      fbd(new double[m_]()), pg(new double[m_ + 1]()), fm(NULL), fb(NULL) {}
+
+void gas_layer_solve::init_fields() {
+    if (sim_ == NULL) fatal_error("gas_layer::init_fields: the gas layer belongs to no simulation", 1);
+    vdi_check(vdi_gas_init_fields(sim_), "vdi_gas_init_fields");
+    pull();
+}
+
+void gas_layer_solve::calc_p_and_tau(double /*t*/, double dt) {
+    vdi_check(vdi_gas_update(sim_, dt), "vdi_gas_update");
+    pull();
+}
+
+void gas_layer_solve::pull() {
+    vdi_check(vdi_sim_synchronize(sim_), "vdi_sim_synchronize");
+    // device arrays by vdi_sim_device_field index, with their host copies
+    struct { int which; double* host; int count; } arr[] = {
+        {5, p, me}, {9, p_old, me}, {10, tau, ml}, {11, tau_old, ml},
+        {3, h, m}, {12, ht, m}, {13, fbd, m}, {4, pg, me}};
+    for (auto& a : arr) {
+        double* d = NULL;
+        size_t count = 0;
+        vdi_check(vdi_sim_device_field(sim_, a.which, &d, &count), "vdi_sim_device_field");
+        if (count != size_t(a.count)) fatal_error("gas_layer: device array of unexpected size", 1);
+        cudaError_t e = cudaMemcpy(a.host, d, count * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) fatal_error(cudaGetErrorString(e), 1);
+    }
+}
 
 gas_layer_solve::~gas_layer_solve() {
     delete[] pg;

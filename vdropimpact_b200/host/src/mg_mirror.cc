@@ -144,8 +144,24 @@ void vdi_tgmg_core::output_res(const char* filename, double ax, double dx, doubl
 }
 
 // ------------------------------------------------------------ problem classes
+// The diagonal reciprocals of the MAC stencil: interior columns with the
+// bottom, middle and top rows, then the side columns with the same rows.
+#define VDI_MAC_RECIPROCALS                                                                  \
+    cc0(-1. / (2 * xxsp + 3 * yysp)), cc1(-1. / (2 * xxsp + 2 * yysp)), cc2(-1. / (2 * xxsp + yysp)), \
+    cc3(-1. / (xxsp + 3 * yysp)), cc4(-1. / (xxsp + 2 * yysp)), cc5(-1. / (xxsp + yysp))
+
+mgs_mac::mgs_mac(fluid_2d& f)
+    : mgs_common(f.m, f.n), xxsp(f.xxsp), yysp(f.yysp), VDI_MAC_RECIPROCALS,
+      acc(tgmg_accuracy(2 * (xxsp + yysp) * f.dt_reg, 1e6)), mg(*this, f.src, z), dx_(f.dx), dy_(f.dy) {
+    mg.setup();
+    mg.clear_z();
+}
+
 mgs_mac::mgs_mac(int m_, int n_, double dx, double dy, double* b)
-    : mgs_common(m_, n_), xxsp(1. / (dx * dx)), yysp(1. / (dy * dy)), acc(0.), mg(*this, b, z), dx_(dx), dy_(dy) {}
+    : mgs_common(m_, n_), xxsp(1. / (dx * dx)), yysp(1. / (dy * dy)), VDI_MAC_RECIPROCALS,
+      acc(tgmg_accuracy(2 * (xxsp + yysp), 1e6)), mg(*this, b, z), dx_(dx), dy_(dy) {}
+
+#undef VDI_MAC_RECIPROCALS
 
 void mgs_mac::solve_v_cycle() {
     double t0 = wtime();
@@ -153,9 +169,43 @@ void mgs_mac::solve_v_cycle() {
     wc_time += wtime() - t0;
 }
 
+// The bilinear element's stencil terms from the spacing ratios.
+#define VDI_FEM_TERMS                                                                              \
+    dydx(dy / dx), dxdy(dx / dy), fm(4. / 3. * (dxdy + dydx)), fm_inv(1.0 / fm),                    \
+    fey(1. / 3. * (-2 * dxdy + dydx)), hey(0.5 * fey), fex(1. / 3. * (-2 * dydx + dxdy)), hex(0.5 * fex), \
+    fc(-1. / 6. * (dxdy + dydx))
+
+mgs_fem::mgs_fem(fluid_2d& f)
+    : mgs_common(f.me, f.ne), dydx(f.dy / f.dx), dxdy(f.dx / f.dy), fm(4. / 3. * (dxdy + dydx)), fm_inv(1.0 / fm),
+      fey(1. / 3. * (-2 * dxdy + dydx)), hey(0.5 * fey), fex(1. / 3. * (-2 * dydx + dxdy)), hex(0.5 * fex),
+      fc(-1. / 6. * (dxdy + dydx)), acc(tgmg_accuracy(fm, 1e8)), mg(*this, f.src, z), dx_(f.dx), dy_(f.dy) {
+    mg.setup();
+    mg.clear_z();
+}
+
 mgs_fem::mgs_fem(int m_, int n_, double dx, double dy, double* b)
-    : mgs_common(m_, n_), dydx(dy / dx), dxdy(dx / dy), fm(4. / 3. * (dxdy + dydx)), acc(0.), mg(*this, b, z),
-      dx_(dx), dy_(dy) {}
+    : mgs_common(m_, n_), VDI_FEM_TERMS, acc(tgmg_accuracy(fm, 1e8)), mg(*this, b, z), dx_(dx), dy_(dy) {}
+
+#undef VDI_FEM_TERMS
+
+double mgs_fem::mul_a(int i, int ij) {
+    if (ij < m) return 0;   // the Dirichlet bottom row
+    const double* w = z + ij;
+    const double* wd = w - m;
+    const bool top = ij >= mn - m;
+    // the row below always couples; the row above only off the top edge,
+    // where the side couplings take the full weight fex instead of hex
+    if (i == 0) {
+        return top ? fc * wd[1] + hey * (*wd) + hex * w[1]
+                   : fc * (wd[1] + w[m + 1]) + hey * (*wd + w[m]) + fex * w[1];
+    }
+    if (i == m - 1) {
+        return top ? fc * wd[-1] + hey * (*wd) + hex * w[-1]
+                   : fc * (wd[-1] + w[m - 1]) + hey * (*wd + w[m]) + fex * w[-1];
+    }
+    return top ? fc * (wd[-1] + wd[1]) + fey * (*wd) + hex * (w[-1] + w[1])
+               : fc * (wd[-1] + wd[1] + w[m - 1] + w[m + 1]) + fey * (*wd + w[m]) + fex * (w[-1] + w[1]);
+}
 
 void mgs_fem::solve_v_cycle() {
     double t0 = wtime();
@@ -164,8 +214,8 @@ void mgs_fem::solve_v_cycle() {
 }
 
 visco_impl::visco_impl(fluid_2d& f, bool horizontal_vel_)
-    : mgs_common(f.m, f.n), x_sym(f.x_sym), horizontal_vel(horizontal_vel_), acc(0.), vfx(0.), vfy(0.),
-      mg(*this, f.src, z) {}
+    : mgs_common(f.m, f.n), x_sym(f.x_sym), horizontal_vel(horizontal_vel_), acc(tgmg_accuracy(1., 1e3)), vfx(0.),
+      vfy(0.), mg(*this, f.src, z) {}
 
 void visco_impl::setup_and_solve(double vfx_, double vfy_, double t) {
     double t0 = wtime();
