@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 namespace vdi {
 
@@ -524,6 +525,251 @@ __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<
     }
 }
 
+// ---------------------------------------- register-blocked cell-centred tile
+// The same window computation as cc_tile (a 64 x 64 window, its halo
+// shrinking one ring per colour phase, the same update and residual
+// arithmetic), laid out so the phases touch no shared memory in the inner
+// loop: thread (warp w, lane t) holds columns 2t, 2t+1 and rows 8w..8w+7 of
+// the window in registers. A red-black update then finds its vertical
+// neighbours in its own registers, one horizontal neighbour in its own other
+// column and the other in the adjacent lane (a shuffle); only each warp's
+// first and last row cross warps, through a small double-buffered shared
+// array, once per phase. The window origin is even, so a thread's 2 x 2
+// blocks are exactly the coarse cells: restriction and the prolongation's
+// coarse neighbourhood stay in registers too.
+template <typename T>
+struct CCReg {
+    static constexpr int R = 8;                 // rows per thread
+    static constexpr int NWARP = 8;
+    static constexpr int NT = 32 * NWARP;
+    static constexpr int CW = 64, CH = R * NWARP;
+    static constexpr int K = 4;                 // colour phases: two red-black sweeps
+    static constexpr int ZH = 6;                // K + 1 rings, rounded up to even
+    static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
+};
+
+/** a[x][y] of a kernel-parameter table. FP32 selects the entry explicitly:
+ * indexing the parameter array with computed indices would copy it to the
+ * stack; FP64 indexes it (the selections would cost registers it lacks). */
+template <typename T>
+__device__ __forceinline__ T pick3(const T (&a)[3][3], int x, int y) {
+    if constexpr (sizeof(T) == 8) {
+        return a[x][y];
+    } else {
+        const T r0 = y == 0 ? a[0][0] : (y == 1 ? a[0][1] : a[0][2]);
+        const T r1 = y == 0 ? a[1][0] : (y == 1 ? a[1][1] : a[1][2]);
+        const T r2 = y == 0 ? a[2][0] : (y == 1 ? a[2][1] : a[2][2]);
+        return x == 0 ? r0 : (x == 1 ? r1 : r2);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename T>
+__device__ __forceinline__ T shfl_dn1(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+/** MODE 0: NS = 2 sweeps from zin (or zero), residual, restriction to bc
+ * (skipped when bc is null). MODE 1: zin + prolonged zc, 2 sweeps, and
+ * optionally the residual norm with the solve decision. Both write zout. */
+template <typename T, int MODE, typename TC = T>
+__global__ void __launch_bounds__(CCReg<T>::NT, 2) cc_rtile(CCc<T> c, TileArgs<T, TC> a) {
+    using G = CCReg<T>;
+    constexpr int R = G::R, CW = G::CW, CH = G::CH, K = G::K, ZH = G::ZH, NWARP = G::NWARP;
+    __shared__ __align__(16) T edge[2][2][NWARP][CW];   // [buffer][first/last row][warp][column]
+    const int m = c.m, n = c.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int zx = blockIdx.x * G::TX - ZH, zy = blockIdx.y * G::TY - ZH;
+    const int i0 = zx + 2 * lane, j0 = zy + warp * R;
+    const bool read_z = MODE == 1 || !a.zero_init;
+    const bool vec = (m & 1) == 0 && ((reinterpret_cast<uintptr_t>(a.zin) | reinterpret_cast<uintptr_t>(a.b) |
+                                       reinterpret_cast<uintptr_t>(a.zout)) & (2 * sizeof(T) - 1)) == 0;
+    using T2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    const bool colin = i0 >= 0 && i0 + 1 < m;
+    T z[R][2], b[R][2];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int j = j0 + r;
+        const bool rowin = unsigned(j) < unsigned(n);
+        if (rowin && colin && vec) {
+            const long o = i0 + long(m) * j;
+            T2 bv = *reinterpret_cast<const T2*>(a.b + o);
+            b[r][0] = bv.x; b[r][1] = bv.y;
+            if (read_z) {
+                T2 zv = *reinterpret_cast<const T2*>(a.zin + o);
+                z[r][0] = zv.x; z[r][1] = zv.y;
+            } else {
+                z[r][0] = z[r][1] = T(0);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int i = i0 + h;
+                const bool in = rowin && unsigned(i) < unsigned(m);
+                b[r][h] = in ? a.b[i + long(m) * j] : T(0);
+                z[r][h] = (in && read_z) ? a.zin[i + long(m) * j] : T(0);
+            }
+        }
+    }
+    if constexpr (MODE == 1) {
+        // prolongation: coarse cell I = i0/2 covers this thread's columns;
+        // fine rows j0..j0+7 use coarse rows J0-1 .. J0+4
+        const int mc = m >> 1, nc = n >> 1, I = i0 >> 1, J0 = j0 >> 1;
+        constexpr int CR = R / 2 + 2;
+        T cm[CR], cc[CR], cp[CR];
+#pragma unroll
+        for (int q = 0; q < CR; q++) {
+            const int J = J0 - 1 + q;
+            const bool rin = unsigned(J) < unsigned(nc);
+            cc[q] = (rin && unsigned(I) < unsigned(mc)) ? T(a.zc[I + long(mc) * J]) : T(0);
+            cm[q] = shfl_up1(cc[q]);
+            cp[q] = shfl_dn1(cc[q]);
+            if (lane == 0) cm[q] = (rin && unsigned(I - 1) < unsigned(mc)) ? T(a.zc[I - 1 + long(mc) * J]) : T(0);
+            if (lane == 31) cp[q] = (rin && unsigned(I + 1) < unsigned(mc)) ? T(a.zc[I + 1 + long(mc) * J]) : T(0);
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int j = j0 + r;
+            const int qJ = 1 + r / 2;                  // coarse row J = j >> 1 in the register window
+            const int sy = (r & 1) ? 1 : -1;           // j0 is even
+            const int Jy = (j >> 1) + sy;
+            const bool yo = Jy < 0 || Jy >= nc;
+            const T gy = T(sy < 0 ? c.gD : c.gU);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int i = i0 + h;
+                if (!(unsigned(i) < unsigned(m) && unsigned(j) < unsigned(n))) continue;
+                const int Ix = I + (h ? 1 : -1);
+                const bool xo = Ix < 0 || Ix >= mc;
+                const T gx = T(h ? c.gR : c.gL);
+                const T c00 = cc[qJ];
+                const T s0 = h ? cp[qJ] : cm[qJ], s1 = h ? cp[qJ + sy] : cm[qJ + sy];
+                const T c10 = xo ? gx * c00 : s0;
+                const T c01 = yo ? gy * c00 : cc[qJ + sy];
+                T c11;
+                if (xo && yo) c11 = gx * gy * c00;
+                else if (xo) c11 = gx * c01;
+                else if (yo) c11 = gy * c10;
+                else c11 = s1;
+                z[r][h] += T(0.5625) * c00 + T(0.1875) * (c10 + c01) + T(0.0625) * c11;
+            }
+        }
+    }
+    // colour phases: colour (i + j) & 1 = col; in row r the thread's point of
+    // that colour is column h = (col + r) & 1 (i0 and j0 are even)
+#pragma unroll
+    for (int ph = 0; ph < K; ph++) {
+        const int col = MODE == 1 ? ((ph & 1) ^ 1) : (ph & 1);
+        T(*eb)[NWARP][CW] = edge[ph & 1];
+        reinterpret_cast<T2*>(&eb[0][warp][0])[lane] = T2{z[0][0], z[0][1]};
+        reinterpret_cast<T2*>(&eb[1][warp][0])[lane] = T2{z[R - 1][0], z[R - 1][1]};
+        __syncthreads();
+        T below[2], above[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            below[h] = warp > 0 ? eb[1][warp - 1][2 * lane + h] : T(0);
+            above[h] = warp < NWARP - 1 ? eb[0][warp + 1][2 * lane + h] : T(0);
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int h = (col + r) & 1;
+            const int j = j0 + r, i = i0 + h;
+            // left and right neighbours: the thread's other column, and the
+            // facing column of the adjacent lane
+            T l, rr;
+            if (h == 0) {
+                l = shfl_up1(z[r][1]);
+                rr = z[r][1];
+            } else {
+                l = z[r][0];
+                rr = shfl_dn1(z[r][0]);
+            }
+            const T d = r > 0 ? z[r > 0 ? r - 1 : 0][h] : below[h];
+            const T u = r < R - 1 ? z[r < R - 1 ? r + 1 : R - 1][h] : above[h];
+            const int ii = 2 * lane + h, jj = warp * R + r;
+            if (ii < ph + 1 || ii > CW - 2 - ph || jj < ph + 1 || jj > CH - 2 - ph) continue;
+            if (!(unsigned(i) < unsigned(m) && unsigned(j) < unsigned(n))) continue;
+            const T xs = (i > 0 ? l : T(0)) + (i < m - 1 ? rr : T(0));
+            const T ys = (j > 0 ? d : T(0)) + (j < n - 1 ? u : T(0));
+            z[r][h] = (b[r][h] - (c.ox * xs + c.oy * ys)) * pick3(c.invd, cls(i, m), cls(j, n));
+        }
+    }
+    // interior back to global memory
+    const bool lanein = 2 * lane >= ZH && 2 * lane < ZH + G::TX;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int jj = warp * R + r, j = j0 + r;
+        if (!lanein || jj < ZH || jj >= ZH + G::TY || j >= n) continue;
+        if (colin && vec) {
+            *reinterpret_cast<T2*>(a.zout + i0 + long(m) * j) = T2{z[r][0], z[r][1]};
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                if (i0 + h < m) a.zout[i0 + h + long(m) * j] = z[r][h];
+        }
+    }
+    const bool want_resid = MODE == 0 ? a.bc != nullptr : a.norm != 0;
+    if (!want_resid) return;
+    // residual of the final iterate at the thread's points (vertical
+    // neighbours across warps once more through the shared array)
+    {
+        T(*eb)[NWARP][CW] = edge[K & 1];
+        reinterpret_cast<T2*>(&eb[0][warp][0])[lane] = T2{z[0][0], z[0][1]};
+        reinterpret_cast<T2*>(&eb[1][warp][0])[lane] = T2{z[R - 1][0], z[R - 1][1]};
+    }
+    __syncthreads();
+    T below[2], above[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        below[h] = warp > 0 ? edge[K & 1][1][warp - 1][2 * lane + h] : T(0);
+        above[h] = warp < NWARP - 1 ? edge[K & 1][0][warp + 1][2 * lane + h] : T(0);
+    }
+    T res[R][2];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int j = j0 + r;
+        const T lft = shfl_up1(z[r][1]), rgt = shfl_dn1(z[r][0]);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int i = i0 + h;
+            const T l = h == 0 ? lft : z[r][0];
+            const T rr = h == 0 ? z[r][1] : rgt;
+            const T d = r > 0 ? z[r > 0 ? r - 1 : 0][h] : below[h];
+            const T u = r < R - 1 ? z[r < R - 1 ? r + 1 : R - 1][h] : above[h];
+            const int ci = cls(i, m), cj = cls(j, n);
+            const T xs = (i > 0 ? l : T(0)) + (i < m - 1 ? rr : T(0));
+            const T ys = (j > 0 ? d : T(0)) + (j < n - 1 ? u : T(0));
+            res[r][h] = b[r][h] - pick3(c.d, ci, cj) * z[r][h] - (c.ox * xs + c.oy * ys);
+        }
+    }
+    if constexpr (MODE == 0) {
+        const int mc = m >> 1, nc = n >> 1, I = i0 >> 1;
+#pragma unroll
+        for (int k = 0; k < R / 2; k++) {
+            const int jj = warp * R + 2 * k, J = (j0 >> 1) + k;
+            if (!lanein || jj < ZH || jj >= ZH + G::TY || unsigned(I) >= unsigned(mc) || unsigned(J) >= unsigned(nc))
+                continue;
+            const T s4 = res[2 * k][0] + res[2 * k][1] + res[2 * k + 1][0] + res[2 * k + 1][1];
+            a.bc[I + long(mc) * J] = TC(T(0.25) * s4);
+        }
+    } else {
+        double s = 0;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int jj = warp * R + r, j = j0 + r;
+            if (!lanein || jj < ZH || jj >= ZH + G::TY || j >= n) continue;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                if (i0 + h >= m) continue;
+                const double rv = double(res[r][h]);
+                s += rv * rv;
+            }
+        }
+        s = block_sum(s);
+        double total;
+        if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
+    }
+}
+
 // -------------------------------------- four-colour split node-centred tile
 // The FEM system's tile: a 64 x 64 window with an even origin, so window point
 // (ii,jj) has colour (ii&1, jj&1); each colour lives in its own 32 x 32
@@ -711,6 +957,241 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
                     s += r * r;
                 }
             }
+        }
+        s = block_sum(s);
+        double total;
+        if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
+    }
+}
+
+// ------------------------------------- register-blocked node-centred tile
+// The FEM counterpart of cc_rtile: the same window computation as fem_tile
+// (64 x 64 nodes, even origin, eight four-colour phases on a shrinking
+// region, the same update, residual and restriction arithmetic), with thread
+// (warp w, lane t) holding columns 2t, 2t+1 and rows 8w..8w+7 in registers.
+// A colour (ci, cj) is column ci of the thread's pair on the rows of parity
+// cj; the eight neighbours are the thread's own registers, the facing
+// column of the adjacent lane (shuffles) and, across warps, the first and
+// last rows through a small shared array.
+template <typename T>
+struct FEMReg {
+    static constexpr int R = 8;
+    static constexpr int NWARP = 8;
+    static constexpr int NT = 32 * NWARP;
+    static constexpr int CW = 64, CH = R * NWARP;
+    static constexpr int K = 8;                 // two four-colour sweeps
+    static constexpr int ZH = 10;               // K + 1 rings, rounded up to even
+    static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
+};
+
+template <typename T, int MODE, typename TC = T>
+__global__ void __launch_bounds__(FEMReg<T>::NT, 2) fem_rtile(FEMc<T> c, TileArgs<T, TC> a) {
+    using G = FEMReg<T>;
+    constexpr int R = G::R, CW = G::CW, CH = G::CH, K = G::K, ZH = G::ZH, NWARP = G::NWARP;
+    __shared__ __align__(16) T edge[2][2][NWARP][CW];
+    const int M = c.M, N = c.N;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int zx = blockIdx.x * G::TX - ZH, zy = blockIdx.y * G::TY - ZH;
+    const int i0 = zx + 2 * lane, j0 = zy + warp * R;
+    const bool read_z = MODE == 1 || !a.zero_init;
+    T z[R][2], b[R][2];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int j = j0 + r;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int i = i0 + h;
+            const bool in = unsigned(j) < unsigned(N) && unsigned(i) < unsigned(M);
+            b[r][h] = in ? a.b[i + long(M) * j] : T(0);
+            z[r][h] = (in && read_z) ? a.zin[i + long(M) * j] : T(0);
+        }
+    }
+    if constexpr (MODE == 1) {
+        // prolongation: coarse node (I, J) sits on fine node (2I, 2J); the
+        // thread's fine rows j0..j0+7 use coarse rows J0..J0+4 of columns I
+        // (its own) and I+1 (the next lane's)
+        const int Mc = (M - 1) / 2 + 1, Nc = (N - 1) / 2 + 1, I = i0 >> 1, J0 = j0 >> 1;
+        constexpr int CR = R / 2 + 1;
+        T cc[CR], cp[CR];
+#pragma unroll
+        for (int q = 0; q < CR; q++) {
+            const int J = J0 + q;
+            const bool rin = unsigned(J) < unsigned(Nc);
+            cc[q] = (rin && unsigned(I) < unsigned(Mc)) ? T(a.zc[I + long(Mc) * J]) : T(0);
+            cp[q] = shfl_dn1(cc[q]);
+            if (lane == 31) cp[q] = (rin && unsigned(I + 1) < unsigned(Mc)) ? T(a.zc[I + 1 + long(Mc) * J]) : T(0);
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int j = j0 + r, q = r >> 1;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int i = i0 + h;
+                if (!(unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N)) || j == 0) continue;
+                const T c00 = cc[q];
+                T v;
+                if (h == 0 && (r & 1) == 0) v = c00;
+                else if (h == 1 && (r & 1) == 0) v = T(0.5) * (c00 + cp[q]);
+                else if (h == 0) v = T(0.5) * (c00 + cc[q + 1]);
+                else v = T(0.25) * (c00 + cp[q] + cc[q + 1] + cp[q + 1]);
+                z[r][h] += v;
+            }
+        }
+    }
+#pragma unroll
+    for (int ph = 0; ph < K; ph++) {
+        const int colour = MODE == 1 ? 3 - (ph & 3) : (ph & 3);
+        const int ci = colour & 1, cj = colour >> 1, oc = 1 - ci;
+        T(*eb)[NWARP][CW] = edge[ph & 1];
+        reinterpret_cast<typename std::conditional<sizeof(T) == 8, double2, float2>::type*>(&eb[0][warp][0])[lane] =
+            {z[0][0], z[0][1]};
+        reinterpret_cast<typename std::conditional<sizeof(T) == 8, double2, float2>::type*>(&eb[1][warp][0])[lane] =
+            {z[R - 1][0], z[R - 1][1]};
+        __syncthreads();
+        T below[2], above[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            below[h] = warp > 0 ? eb[1][warp - 1][2 * lane + h] : T(0);
+            above[h] = warp < NWARP - 1 ? eb[0][warp + 1][2 * lane + h] : T(0);
+        }
+        // the other column of the thread (rows -1..R) and the facing column
+        // of the adjacent lane: left of column 0, right of column 1
+        T own[R + 2], nb[R + 2];
+#pragma unroll
+        for (int k = 0; k < R + 2; k++) {
+            own[k] = k == 0 ? below[oc] : (k == R + 1 ? above[oc] : z[k == 0 || k == R + 1 ? 0 : k - 1][oc]);
+            nb[k] = ci == 0 ? shfl_up1(own[k]) : shfl_dn1(own[k]);
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            if ((r & 1) != cj) continue;
+            const int i = i0 + ci, j = j0 + r;
+            const int ii = 2 * lane + ci, jj = warp * R + r;
+            const T d = r > 0 ? z[r > 0 ? r - 1 : 0][ci] : below[ci];
+            const T u = r < R - 1 ? z[r < R - 1 ? r + 1 : R - 1][ci] : above[ci];
+            // rows r-1, r, r+1 sit at k = r, r+1, r+2 of own[] and nb[]
+            const T l = ci == 0 ? nb[r + 1] : own[r + 1];
+            const T rr = ci == 0 ? own[r + 1] : nb[r + 1];
+            const T dl = ci == 0 ? nb[r] : own[r];
+            const T dr = ci == 0 ? own[r] : nb[r];
+            const T ul = ci == 0 ? nb[r + 2] : own[r + 2];
+            const T ur = ci == 0 ? own[r + 2] : nb[r + 2];
+            if (ii < ph + 1 || ii > CW - 2 - ph || jj < ph + 1 || jj > CH - 2 - ph) continue;
+            if (!(unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N))) continue;
+            z[r][ci] = (b[r][ci] - fem_off_vals(c, i, j, dl, d, dr, l, rr, ul, u, ur)) *
+                       pick3(c.invd, cls(i, M), cls(j, N));
+        }
+    }
+    const bool lanein = 2 * lane >= ZH && 2 * lane < ZH + G::TX;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int jj = warp * R + r, j = j0 + r;
+        if (!lanein || jj < ZH || jj >= ZH + G::TY || j >= N) continue;
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+            if (i0 + h < M) a.zout[i0 + h + long(M) * j] = z[r][h];
+    }
+    const bool want_resid = MODE == 0 ? a.bc != nullptr : a.norm != 0;
+    if (!want_resid) return;
+    // the final iterate's first and last rows across warps once more
+    {
+        T(*eb)[NWARP][CW] = edge[K & 1];
+        eb[0][warp][2 * lane] = z[0][0];
+        eb[0][warp][2 * lane + 1] = z[0][1];
+        eb[1][warp][2 * lane] = z[R - 1][0];
+        eb[1][warp][2 * lane + 1] = z[R - 1][1];
+    }
+    __syncthreads();
+    T below[2], above[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        below[h] = warp > 0 ? edge[K & 1][1][warp - 1][2 * lane + h] : T(0);
+        above[h] = warp < NWARP - 1 ? edge[K & 1][0][warp + 1][2 * lane + h] : T(0);
+    }
+    // residual of row r at both columns
+    auto zrow = [&](int k, int h) -> T { return k < 0 ? below[h] : (k >= R ? above[h] : z[k < 0 ? 0 : (k >= R ? R - 1 : k)][h]); };
+    auto resid_row = [&](int r, T& r0, T& r1) {
+        const int j = j0 + r;
+        const T up1 = shfl_up1(zrow(r, 1)), up1d = shfl_up1(zrow(r - 1, 1)), up1u = shfl_up1(zrow(r + 1, 1));
+        const T dn0 = shfl_dn1(zrow(r, 0)), dn0d = shfl_dn1(zrow(r - 1, 0)), dn0u = shfl_dn1(zrow(r + 1, 0));
+        {
+            const int i = i0;
+            const T off = fem_off_vals(c, i, j, up1d, zrow(r - 1, 0), zrow(r - 1, 1), up1, zrow(r, 1), up1u,
+                                       zrow(r + 1, 0), zrow(r + 1, 1));
+            r0 = b[r][0] - pick3(c.d, cls(i, M), cls(j, N)) * z[r][0] - off;
+        }
+        {
+            const int i = i0 + 1;
+            const T off = fem_off_vals(c, i, j, zrow(r - 1, 0), zrow(r - 1, 1), dn0d, zrow(r, 0), dn0,
+                                       zrow(r + 1, 0), zrow(r + 1, 1), dn0u);
+            r1 = b[r][1] - pick3(c.d, cls(i, M), cls(j, N)) * z[r][1] - off;
+        }
+        const bool rowin = unsigned(j) < unsigned(N);
+        if (!(rowin && unsigned(i0) < unsigned(M))) r0 = T(0);
+        if (!(rowin && unsigned(i0 + 1) < unsigned(M))) r1 = T(0);
+    };
+    if constexpr (MODE == 0) {
+        // P^T: coarse node (I, J) on fine (2I, 2J) gathers rows 2J-1..2J+1
+        // and columns 2I-1..2I+1 (half weights off the centre line); the row
+        // below the strip comes from the warp below, the column left of the
+        // thread's pair from the adjacent lane
+        __shared__ T rlast[NWARP][CW];
+        T rl0, rl1;
+        resid_row(R - 1, rl0, rl1);
+        rlast[warp][2 * lane] = rl0;
+        rlast[warp][2 * lane + 1] = rl1;
+        __syncthreads();
+        T pr0 = warp > 0 ? rlast[warp - 1][2 * lane] : T(0);
+        T pr1 = warp > 0 ? rlast[warp - 1][2 * lane + 1] : T(0);
+        const int Mc = (M - 1) / 2 + 1, Nc = (N - 1) / 2 + 1, I = i0 >> 1;
+#pragma unroll
+        for (int k = 0; k < R / 2; k++) {
+            T c0, c1, n0, n1;
+            resid_row(2 * k, c0, c1);
+            if (2 * k + 1 == R - 1) {
+                n0 = rl0;
+                n1 = rl1;
+            } else {
+                resid_row(2 * k + 1, n0, n1);
+            }
+            // column 2I-1: the previous lane's second column
+            const T pl = shfl_up1(pr1), cl = shfl_up1(c1), nl = shfl_up1(n1);
+            const int jj = warp * R + 2 * k, J = (j0 >> 1) + k;
+            const bool ok = lanein && jj >= ZH && jj < ZH + G::TY && unsigned(I) < unsigned(Mc) &&
+                            unsigned(J) < unsigned(Nc);
+            if (ok) {
+                T sum = 0;
+                if (J > 0) {
+                    const T rows[3][3] = {{pl, pr0, pr1}, {cl, c0, c1}, {nl, n0, n1}};
+#pragma unroll
+                    for (int dj = -1; dj <= 1; dj++) {
+                        const int jf = 2 * J + dj;
+                        if (jf < 0 || jf >= N) continue;
+                        const T wy = dj == 0 ? T(1) : T(0.5);
+#pragma unroll
+                        for (int di = -1; di <= 1; di++) {
+                            const int ifn = 2 * I + di;
+                            if (ifn < 0 || ifn >= M) continue;
+                            const T wx = di == 0 ? T(1) : T(0.5);
+                            sum += wx * wy * rows[dj + 1][di + 1];
+                        }
+                    }
+                }
+                a.bc[I + long(Mc) * J] = TC(sum);
+            }
+            pr0 = n0;
+            pr1 = n1;
+        }
+    } else {
+        double s = 0;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            T r0, r1;
+            resid_row(r, r0, r1);
+            const int jj = warp * R + r, j = j0 + r;
+            if (!lanein || jj < ZH || jj >= ZH + G::TY || j >= N) continue;
+            if (i0 < M) s += double(r0) * double(r0);
+            if (i0 + 1 < M) s += double(r1) * double(r1);
         }
         s = block_sum(s);
         double total;
@@ -1102,8 +1583,25 @@ struct LevelD {
     signed char gL, gR, gD, gU;
 };
 
+/** Which cell-centred tile kernel the V-cycles launch: the shared-memory
+ * one (default) or the register-blocked one (VDI_MG_TILE=reg), read once. */
+static bool use_reg_tile() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("VDI_MG_TILE");
+        v = (e && std::strcmp(e, "reg") == 0) ? 1 : 0;
+    }
+    return v == 1;
+}
+
 template <typename T, int MODE, typename TC = T>
 static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T, TC>& a) {
+    if (use_reg_tile()) {
+        using G = CCReg<T>;
+        dim3 grid((c.m + G::TX - 1) / G::TX, (c.n + G::TY - 1) / G::TY);
+        cc_rtile<T, MODE, TC><<<grid, G::NT, 0, s>>>(c, a);
+        return;
+    }
     using G = CCTile<T, 2>;
     dim3 grid((c.m + G::TX - 1) / G::TX, (c.n + G::TY - 1) / G::TY);
     cc_tile<T, MODE, 2, TC><<<grid, G::NT, G::smem, s>>>(c, a);
@@ -1111,6 +1609,12 @@ static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T, TC
 
 template <typename T, int MODE, typename TC = T>
 static void launch_fem_tile(cudaStream_t s, const FEMc<T>& c, const TileArgs<T, TC>& a) {
+    if (use_reg_tile()) {
+        using G = FEMReg<T>;
+        dim3 grid((c.M + G::TX - 1) / G::TX, (c.N + G::TY - 1) / G::TY);
+        fem_rtile<T, MODE, TC><<<grid, G::NT, 0, s>>>(c, a);
+        return;
+    }
     using G = FEMTile<T>;
     dim3 grid((c.M + G::TX - 1) / G::TX, (c.N + G::TY - 1) / G::TY);
     fem_tile<T, MODE, TC><<<grid, G::NT, G::smem, s>>>(c, a);
