@@ -383,6 +383,13 @@ int vdi_unet_params(vdi_unet* net, float* h_buf, long count, int to_device);
  * out_scale * rms(residual) / xxsp, prolonged back, is added to the guess. */
 int vdi_sim_attach_unet(vdi_sim* sim, vdi_unet* net, int factor, double out_scale);
 
+/* The learned guess for a standalone MAC solve (no reference counterpart):
+ * with r = b - A z for the current z, adds to z the network's prediction of
+ * A^-1 r: r restricted by factor and divided by its RMS is the input, and
+ * the output times scale * rms(r), prolonged back, is the correction (scale
+ * is the network's output scale over xxsp). Then solve from z as usual. */
+int vdi_unet_guess(vdi_unet* net, vdi_mg* mg, int factor, double scale, const double* d_b, double* d_z);
+
 /* vdi_mg_solve_noalloc has no counterpart in the reference. It is an FP64
  * multigrid solve of the systems of vdi_mg_create + vdi_mg_solve for callers
  * that must not allocate device memory, such as an application that owns

@@ -123,6 +123,7 @@ _SIGS = [
     ("vdi_sim_device_field", C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(C.c_size_t)]),
     ("vdi_sim_vcycle_bytes", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     ("vdi_sim_get_params", C.c_int, [C.c_void_p, C.POINTER(VdiParams)]),
+    ("vdi_unet_guess", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     ("vdi_sim_init_tracers", C.c_int, [C.c_void_p]),
     ("vdi_sim_update_tracers", C.c_int, [C.c_void_p, C.c_double]),
     ("vdi_sim_set_nif_mode", C.c_int, [C.c_void_p, C.c_int, C.c_double]),

@@ -1432,6 +1432,10 @@ __device__ __forceinline__ void grid_walk(int m, long tot, F f) {
     if (k >= tot) return;
     int j = int(k / m), i = int(k - long(j) * m);
     const int sj = int(stride / m), si = int(stride - long(sj) * m);
+    // unrolled so that later points' loads issue before earlier points'
+    // arithmetic: a thread walks several points, and one load at a time
+    // leaves the memory system idle
+#pragma unroll 4
     for (; k < tot; k += stride) {
         f(k, i, j);
         i += si;
@@ -2387,6 +2391,11 @@ int mg_tiled_levels(const MG* mg, int precision) {
 SolveCtl* mg_ctl(MG* mg) { return mg->ctl; }
 int mg_kind(const MG* mg) { return mg->kind; }
 int mg_fine_size(const MG* mg) { return int(mg->size(0)); }
+int mg_dims(const MG* mg, int* m, int* n) {
+    *m = mg->m;
+    *n = mg->n;
+    return VDI_OK;
+}
 
 int mg_configure(MG* mg, double rtol, int max_it) { return mg->set_ctl_params(0, rtol, max_it); }
 

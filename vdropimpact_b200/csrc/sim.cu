@@ -1049,6 +1049,33 @@ int vdi_mg_apply(vdi_mg* h, const double* d_z, double* d_y) {
     return VDI_OK;
 }
 
+int vdi_unet_guess(vdi_unet* net, vdi_mg* h, int factor, double scale, const double* d_b, double* d_z) {
+    if (!net || !h || !d_b || !d_z || (factor != 1 && factor != 2 && factor != 4 && factor != 8))
+        return VDI_ERR_INVALID_ARGUMENT;
+    const int kind = mg_kind(h->g);
+    if (kind != VDI_MG_MAC && kind != VDI_MG_MAC_NEUMANN) {
+        set_error("vdi_unet_guess: the learned guess is defined for the cell-centred MAC system");
+        return VDI_ERR_INVALID_ARGUMENT;
+    }
+    int H, W;
+    unet_dims(net, &H, &W);
+    const long mn = mg_fine_size(h->g);
+    cudaStream_t s = h->s;
+    double* r = nullptr;
+    float* io = nullptr;
+    VDI_CUDA(cudaMallocAsync(&r, sizeof(double) * (mn + 1), s));
+    VDI_CUDA(cudaMallocAsync(&io, sizeof(float) * 2 * size_t(H) * W, s));
+    int st = mg_residual_async(h->g, s, d_b, d_z, r, r + mn);
+    int m = 0, n = 0;
+    if (st == VDI_OK) st = mg_dims(h->g, &m, &n);
+    if (st == VDI_OK) st = unet_correct(net, s, r, r + mn, d_z, m, n, factor, scale, io, io + size_t(H) * W);
+    cudaFreeAsync(io, s);
+    cudaFreeAsync(r, s);
+    VDI_TRY(st);
+    VDI_CUDA(cudaStreamSynchronize(s));
+    return VDI_OK;
+}
+
 int vdi_mg_coarse_cycle(const vdi_mg* h, int precision, int* first_level, int* ctas) {
     if (!h || !first_level || !ctas) return VDI_ERR_INVALID_ARGUMENT;
     return mg_coarse_cycle(h->g, precision, first_level, ctas);

@@ -704,11 +704,26 @@ __global__ void k_frame_apply(double* __restrict__ v, long tot, const double* __
 // The target time is *d_time + tadd: a guess enqueued before the kernel that
 // advances the clock by dt/2 passes tadd = dt/2 and gets the same double that
 // the clock will hold (the same single rounded addition).
+/** Points per thread of k_guess. */
+static constexpr int GUESS_PER = 4;
+
 template <bool QUAD>
 __global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, double* __restrict__ zprev2, int n,
                         GuessHist* h, const double* d_time, double tadd, int* err) {
     __shared__ double s_t[4];   // t, t0, t_prev, t_prev2
     __shared__ int s_sc, s_head;
+    // each thread takes GUESS_PER points, a grid-size apart; their values
+    // are loaded before the history header is, so the two overlap
+    const int k0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    double vz[GUESS_PER], va[GUESS_PER], vb[GUESS_PER];
+#pragma unroll
+    for (int u = 0; u < GUESS_PER; u++) {
+        const int k = k0 + u * stride;
+        const bool in = k < n;
+        vz[u] = in ? z[k] : 0.;
+        va[u] = in ? zprev[k] : 0.;
+        vb[u] = (QUAD && in) ? zprev2[k] : 0.;
+    }
     if (threadIdx.x == 0) {
         s_t[0] = *d_time + tadd;
         s_t[1] = h->t0;
@@ -723,23 +738,27 @@ __global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, doub
     const bool dup = fabs(t0 - t1) < 2.220446049250313e-16 * 10;
     // quadratic history: h1 holds the solution at t_prev, h2 the one at
     // t_prev2; the newest history replaces h2's and the two swap roles
-    double* h1 = (QUAD && s_head) ? zprev2 : zprev;
-    double* h2 = (QUAD && s_head) ? zprev : zprev2;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) {
+    const bool swap = QUAD && s_head;
+    double* h1 = swap ? zprev2 : zprev;
+    double* h2 = swap ? zprev : zprev2;
+#pragma unroll
+    for (int u = 0; u < GUESS_PER; u++) {
+        const int k = k0 + u * stride;
+        if (k >= n) continue;
+        const double v1 = swap ? vb[u] : va[u], v2 = swap ? va[u] : vb[u];
         if (sc < 2) {
-            if (sc == 1) h1[k] = z[k];
+            if (sc == 1) h1[k] = vz[u];
         } else if (!dup) {
-            double zz = z[k];
+            double zz = vz[u];
             if (!QUAD || sc == 2) {
                 double a = 1. / (t0 - t1), b = (t - t1) * a, cc = (t - t0) * a;
-                z[k] = b * zz - cc * h1[k];
+                z[k] = b * zz - cc * v1;
             } else {
                 double t2 = s_t[3];
                 double l0 = (t - t1) * (t - t2) / ((t0 - t1) * (t0 - t2));
                 double l1 = (t - t0) * (t - t2) / ((t1 - t0) * (t1 - t2));
                 double l2 = (t - t0) * (t - t1) / ((t2 - t0) * (t2 - t1));
-                z[k] = l0 * zz + l1 * h1[k] + l2 * h2[k];
+                z[k] = l0 * zz + l1 * v1 + l2 * v2;
             }
             if (QUAD) h2[k] = zz;
             else h1[k] = zz;
@@ -853,9 +872,11 @@ int launch_guess(cudaStream_t s, double* z, double* zprev, double* zprev2, int n
                  const double* d_time, double tadd, int quadratic, int* err) {
     if (n <= 0) return VDI_OK;
     if (quadratic)
-        k_guess<true><<<(n + 255) / 256, 256, 0, s>>>(z, zprev, zprev2, n, h, d_time, tadd, err);
+        k_guess<true><<<(n + 256 * GUESS_PER - 1) / (256 * GUESS_PER), 256, 0, s>>>(z, zprev, zprev2, n, h, d_time,
+                                                                                     tadd, err);
     else
-        k_guess<false><<<(n + 255) / 256, 256, 0, s>>>(z, zprev, zprev2, n, h, d_time, tadd, err);
+        k_guess<false><<<(n + 256 * GUESS_PER - 1) / (256 * GUESS_PER), 256, 0, s>>>(z, zprev, zprev2, n, h, d_time,
+                                                                                      tadd, err);
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 

@@ -117,6 +117,7 @@ int mg_apply(MG* mg, cudaStream_t s, const double* z, double* y);
 SolveCtl* mg_ctl(MG* mg);          // device pointer
 int mg_kind(const MG* mg);
 int mg_fine_size(const MG* mg);    // number of unknowns on the finest level
+int mg_dims(const MG* mg, int* m, int* n);   // finest level: cells (MAC, viscous) or nodes (FEM)
 /** Configures the device-controlled solve (rtol, V-cycle cap). */
 int mg_configure(MG* mg, double rtol, int max_it);
 /** Builds the conditional-node loop for the solve into a graph under
