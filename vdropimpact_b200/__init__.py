@@ -506,6 +506,7 @@ class MgsMac(_MgSystem):
 
     def __init__(self, m, n, dx, dy, stream=None):
         super().__init__(m, n, dx, dy, False, stream)
+        self.xxsp, self.yysp = 1. / (dx * dx), 1. / (dy * dy)
 
 
 class MgsMacNeumann(_MgSystem):

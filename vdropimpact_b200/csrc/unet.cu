@@ -23,6 +23,7 @@
 
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <type_traits>
 
 #include <cmath>
 #include <cstring>
@@ -181,6 +182,223 @@ __global__ void __launch_bounds__(256) conv3x3_k(ConvArgs<TIN, TOUT> a) {
         }
     }
 }
+
+// ------------------------------------------- Blackwell tensor-core path
+// The same convolution on the fifth-generation tensor cores: tcgen05.mma with
+// both operands in shared memory and the FP32 accumulator in tensor memory.
+// One CTA of four warps takes a row segment of TC_M = 128 output pixels
+// (the MMA's M), so the A operand of tap (dy, dx) is a window of the staged
+// input rows shifted by whole pixels: a pixel's 8-channel chunk is one
+// 16-byte core-matrix row, 8 consecutive pixels one 8 x 16-byte core
+// matrix, and the operand needs no copy per tap. The weights, already stored
+// [tap][cout][cin], are K-major B operands. A CTA stages the weights once and
+// then walks its row segments; each segment is 9 * CIN/16 MMAs (K = 16
+// each) into one accumulator, read back with tcgen05.ld for the bias,
+// skip-add, ReLU epilogue.
+namespace tc {
+
+constexpr int TC_M = 128;            // output pixels per segment (MMA M)
+constexpr int TC_PX = TC_M + 2;      // staged pixels per input row (one halo pixel each side)
+constexpr int TC_THREADS = 128;
+
+__device__ int g_timeout;            // set when a bounded wait gave up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+/** Shared-memory matrix descriptor of a K-major operand without swizzle:
+ * core matrices of 8 rows x 16 bytes, lbo the byte distance between the two
+ * core matrices of one K = 16 step, sbo between consecutive 8-row groups. */
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = uint64_t((addr >> 4) & 0x3FFFu);
+    d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+    d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+    d |= uint64_t(1) << 46;          // descriptor version of sm_100
+    return d;                         // base offset 0, no swizzle
+}
+
+/** Instruction descriptor of kind::f16: BF16 A and B, both K-major, FP32 D,
+ * M x N. */
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16_ss(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+/** Waits for the mbarrier phase with a time limit (about 0.5 s of SM
+ * clock); false if it gave up. */
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > 1000000000LL) return false;
+    }
+}
+
+/** 16 consecutive FP32 accumulator columns of this thread's TMEM lane. */
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+}
+
+template <int CIN, int COUT>
+constexpr size_t tc_smem() {
+    return size_t(9) * (CIN / 8) * COUT * 16 + size_t(3) * (CIN / 8) * TC_PX * 16;
+}
+
+template <int CIN, int COUT, typename TIN, typename TOUT>
+__global__ void __launch_bounds__(TC_THREADS) conv3x3_tc(ConvArgs<TIN, TOUT> a) {
+    constexpr int KC = CIN / 8;                              // 16-byte channel chunks
+    constexpr uint32_t CHUNKB = uint32_t(TC_PX) * 16;        // one chunk of one staged row
+    constexpr uint32_t ROWB = uint32_t(KC) * CHUNKB;         // one staged row, all chunks
+    constexpr uint32_t WTAPB = uint32_t(KC) * COUT * 16;     // one tap of weights
+    constexpr int TCOLS = COUT < 32 ? 32 : COUT;             // TMEM columns (a power of two, >= 32)
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "tcgen05 shape");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* wsm = smem;                               // [9][KC][COUT][8] bf16
+    unsigned char* rows = smem + 9 * WTAPB;                  // [3][KC][TC_PX][8] bf16
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int q = tid; q < 9 * COUT * KC; q += TC_THREADS) {
+        const int kc = q % KC, co = (q / KC) % COUT, t = q / (KC * COUT);
+        *reinterpret_cast<uint4*>(wsm + (uint32_t(t) * KC + kc) * COUT * 16 + co * 16) =
+            *reinterpret_cast<const uint4*>(a.w + (size_t(t) * COUT + co) * CIN + kc * 8);
+    }
+    const uint32_t bar_a = smem_u32(&bar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+    constexpr uint32_t IDESC = idesc_bf16(TC_M, COUT);
+    const int segs = (a.W + TC_M - 1) / TC_M;
+    const long tasks = long(a.B) * a.H * segs;
+    uint32_t phase = 0;
+    int ok = 1;
+    for (long task = blockIdx.x; task < tasks && ok; task += gridDim.x) {
+        const int seg = int(task % segs);
+        const long r = task / segs;
+        const int y = int(r % a.H), b = int(r / a.H), x0 = seg * TC_M;
+        // input rows y-1..y+1, pixels x0-1..x0+TC_M, as 16-byte channel chunks
+        for (int q = tid; q < 3 * KC * TC_PX; q += TC_THREADS) {
+            const int px = q % TC_PX, kc = (q / TC_PX) % KC, row = q / (TC_PX * KC);
+            const int yy = y + row - 1, xx = x0 + px - 1;
+            uint4 v;
+            if (std::is_same<TIN, bf16>::value && a.mode == SRC_DIRECT && !a.mask) {
+                const bool in = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+                v = in ? *reinterpret_cast<const uint4*>(a.src + ((size_t(b) * a.H + yy) * a.W + xx) * CIN + kc * 8)
+                       : make_uint4(0, 0, 0, 0);
+            } else {
+                __align__(16) bf16 e[8];
+#pragma unroll
+                for (int c = 0; c < 8; c++)
+                    e[c] = __float2bfloat16(src_at(a.src, a.mask, a.mode, a.H, a.W, CIN, b, yy, xx, kc * 8 + c));
+                v = *reinterpret_cast<const uint4*>(e);
+            }
+            *reinterpret_cast<uint4*>(rows + uint32_t(row) * ROWB + uint32_t(kc) * CHUNKB + uint32_t(px) * 16) = v;
+        }
+        fence_async_smem();   // the staged rows (and weights) become visible to the tensor cores
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (tid == 0) {
+            uint32_t acc = 0;
+#pragma unroll 1
+            for (int t = 0; t < 9; t++) {
+                const int dy = t / 3, dx = t % 3;
+#pragma unroll
+                for (int kb = 0; kb < CIN / 16; kb++) {
+                    const uint32_t aa = smem_u32(rows + uint32_t(dy) * ROWB + uint32_t(2 * kb) * CHUNKB + dx * 16);
+                    const uint32_t ba = smem_u32(wsm + uint32_t(t) * WTAPB + uint32_t(2 * kb) * COUT * 16);
+                    mma_bf16_ss(tmem, sdesc(aa, CHUNKB, 128), sdesc(ba, uint32_t(COUT) * 16, 128), IDESC, acc);
+                    acc = 1;
+                }
+            }
+            mma_commit(bar_a);
+        }
+        ok = mbar_wait(bar_a, phase) ? 1 : 0;
+        phase ^= 1;
+        ok = __syncthreads_and(ok);
+        fence_after();
+        if (ok) {
+            const int x = x0 + warp * 32 + lane;
+            const uint32_t ta = tmem + (uint32_t(warp * 32) << 16);
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                float v[16];
+                tmem_ld16(ta + c0, v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (x < a.W) {
+                    const size_t k = ((size_t(b) * a.H + y) * a.W + x) * COUT + c0;
+#pragma unroll
+                    for (int c = 0; c < 16; c++) {
+                        float w = v[c];
+                        if (a.bias) w += a.bias[c0 + c];
+                        if (a.resid) w += __bfloat162float(a.resid[k + c]);
+                        if (a.relu) w = fmaxf(w, 0.f);
+                        a.out[k + c] = from_f<TOUT>(w);
+                    }
+                }
+            }
+        }
+        fence_before();
+        __syncthreads();   // accumulator read and staged rows consumed before the next segment
+        fence_after();
+    }
+    if (!ok) {
+        // a wait gave up: note it, and give any MMA still in flight a bounded
+        // time to finish before the tensor memory is released
+        if (tid == 0) {
+            atomicExch(&g_timeout, 1);
+            (void)mbar_wait(bar_a, phase ^ 1);
+        }
+        __syncthreads();
+    }
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
+}
+
+}  // namespace tc
 
 template <int CIN, int COUT>
 constexpr size_t conv_smem() {
@@ -392,8 +610,32 @@ struct Net {
     int step = 0;
 };
 
+/** Whether the convolutions run on tcgen05 (VDI_UNET_TC=1) or mma.sync. */
+static bool use_tc() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("VDI_UNET_TC");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v == 1;
+}
+
 template <int CIN, int COUT, typename TIN, typename TOUT>
 static cudaError_t conv_launch(cudaStream_t s, const ConvArgs<TIN, TOUT>& a) {
+    if (use_tc()) {
+        static bool tattr = false;
+        if (!tattr) {
+            cudaError_t e = cudaFuncSetAttribute(tc::conv3x3_tc<CIN, COUT, TIN, TOUT>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 int(tc::tc_smem<CIN, COUT>()));
+            if (e != cudaSuccess) return e;
+            tattr = true;
+        }
+        const long tasks = long(a.B) * a.H * ((a.W + tc::TC_M - 1) / tc::TC_M);
+        const int grid = int(tasks < 296 ? tasks : 296);
+        tc::conv3x3_tc<CIN, COUT, TIN, TOUT><<<grid, tc::TC_THREADS, tc::tc_smem<CIN, COUT>(), s>>>(a);
+        return cudaGetLastError();
+    }
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(conv3x3_k<CIN, COUT, TIN, TOUT>,
@@ -608,6 +850,20 @@ long vdi_unet_param_count(const vdi_unet* u) {
     return c;
 }
 
+/** Reports a tensor-core wait that gave up (the kernels return without
+ * their result rather than wait longer). */
+static int tc_status(cudaStream_t s) {
+    if (!use_tc()) return VDI_OK;
+    int t = 0;
+    VDI_CUDA(cudaMemcpyFromSymbolAsync(&t, tc::g_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+    VDI_CUDA(cudaStreamSynchronize(s));
+    if (t) {
+        set_error("unet: a tensor-core convolution timed out waiting for its MMAs");
+        return VDI_ERR_CUDA;
+    }
+    return VDI_OK;
+}
+
 int vdi_unet_forward(vdi_unet* u, const float* d_in, float* d_out, int batch) {
     if (!u || !d_in || !d_out || batch < 1 || batch > u->net->Bmax) return VDI_ERR_INVALID_ARGUMENT;
     Net* n = u->net;
@@ -616,7 +872,7 @@ int vdi_unet_forward(vdi_unet* u, const float* d_in, float* d_out, int batch) {
     VDI_TRY(net_forward(n, u->s, batch, true));
     unpack_output_k<<<592, 256, 0, u->s>>>(n->outf, d_out, npx);
     VDI_CUDA(cudaGetLastError());
-    return VDI_OK;
+    return tc_status(u->s);
 }
 
 int vdi_unet_train_step(vdi_unet* u, const float* d_in, const float* d_target, int batch, float lr, float* loss) {
@@ -645,7 +901,7 @@ int vdi_unet_train_step(vdi_unet* u, const float* d_in, const float* d_target, i
         VDI_CUDA(cudaMemcpyAsync(loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
         VDI_CUDA(cudaStreamSynchronize(s));
     }
-    return VDI_OK;
+    return tc_status(s);
 }
 
 /** Gradient check support: forward + loss + backward without an update;
