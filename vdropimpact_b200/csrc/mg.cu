@@ -155,7 +155,10 @@ __device__ void solve_decide(SolveCtl* ctl, double r2, int count_cycle, int use_
             cont = 1;
         }
     }
-    if (ctl->status) ctl->sticky |= ctl->status;
+    if (ctl->status) {
+        ctl->sticky |= ctl->status;
+        if (ctl->err_out) atomicOr(ctl->err_out, ctl->status);
+    }
     if (!cont) {
         ctl->done = 1;
         ctl->solves += 1;
@@ -2318,9 +2321,12 @@ class MG {
         static_assert(offsetof(SolveCtl, it) + sizeof(int) == offsetof(SolveCtl, max_it), "layout");
         VDI_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(ctl) + offsetof(SolveCtl, rtol), &p,
                                  sizeof(double) + 2 * sizeof(int), cudaMemcpyHostToDevice, s));
+        VDI_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(ctl) + offsetof(SolveCtl, err_out), &err_word,
+                                 sizeof(int*), cudaMemcpyHostToDevice, s));
         VDI_CUDA(cudaStreamSynchronize(s));
         return VDI_OK;
     }
+    int* err_word = nullptr;   // see mg_set_error_word
 };
 
 int mg_create(int kind, int m, int n, double c1, double c2, int x_sym, MG** out) {
@@ -2398,6 +2404,10 @@ int mg_dims(const MG* mg, int* m, int* n) {
 }
 
 int mg_configure(MG* mg, double rtol, int max_it) { return mg->set_ctl_params(0, rtol, max_it); }
+int mg_set_error_word(MG* mg, int* d_err) {
+    mg->err_word = d_err;
+    return mg->set_ctl_params(0, mg->rtol, mg->max_it);
+}
 
 int mg_solve(MG* mg, cudaStream_t s, const double* b, double* z, double rtol, int max_it, int precision,
              int* vcycles, double* rel_res) {

@@ -210,15 +210,11 @@ int enqueue_step(vdi_sim* S, double dt) {
 }
 
 int check_errors(vdi_sim* S) {
+    // one word: the step's kernels and every solve (mg_set_error_word) OR
+    // their failure bits into it
     int err = 0;
+    VDI_CUDA(cudaMemcpyAsync(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, S->s));
     VDI_CUDA(cudaStreamSynchronize(S->s));
-    VDI_CUDA(cudaMemcpy(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < 4; k++) {
-        if (!S->mg[k]) continue;
-        SolveCtl c;
-        VDI_CUDA(cudaMemcpy(&c, mg_ctl(S->mg[k]), sizeof(SolveCtl), cudaMemcpyDeviceToHost));
-        err |= c.sticky;
-    }
     if (err & DEV_NONFINITE) {
         set_error("non-finite value in a residual");
         return VDI_ERR_NONFINITE;
@@ -560,7 +556,8 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
         if ((st = mg_create(VDI_MG_VISC_V, m, n, 1., 1., P.x_sym, &S->mg[SOLVER_VY])) != VDI_OK) return fail(st);
     }
     for (int k = 0; k < 4; k++)
-        if (S->mg[k] && (st = mg_configure(S->mg[k], S->prm.mg_rtol, S->prm.mg_max_vcycles)) != VDI_OK)
+        if (S->mg[k] && ((st = mg_configure(S->mg[k], S->prm.mg_rtol, S->prm.mg_max_vcycles)) != VDI_OK ||
+                         (st = mg_set_error_word(S->mg[k], S->d_err)) != VDI_OK))
             return fail(st);
     double* lbuf;
     if ((st = alloc_zero(S, &lbuf, sizeof(LiftoffState) / 8 + 1)) != VDI_OK) return fail(st);

@@ -54,6 +54,7 @@ struct SolveCtl {
     long long vcycles;
     double last_rel;
     int sticky;         // DevErr bits of every solve since creation
+    int* err_out;       // when set, a failing solve also ORs its bits here
 };
 
 /** Deterministic block-then-grid sum: each block writes one partial, the
@@ -120,6 +121,9 @@ int mg_fine_size(const MG* mg);    // number of unknowns on the finest level
 int mg_dims(const MG* mg, int* m, int* n);   // finest level: cells (MAC, viscous) or nodes (FEM)
 /** Configures the device-controlled solve (rtol, V-cycle cap). */
 int mg_configure(MG* mg, double rtol, int max_it);
+/** A device word that failing solves OR their DevErr bits into (the
+ * owner's error word), kept across rebuilds of the hierarchy. */
+int mg_set_error_word(MG* mg, int* d_err);
 /** Builds the conditional-node loop for the solve into a graph under
  * stream capture. Returns VDI_OK when a graph loop was recorded. */
 int mg_record_graph_solve(MG* mg, cudaStream_t s, const double* b, double* z, int precision);
