@@ -31,10 +31,15 @@ def cfg_text(m=256, n=128, drop=()):
 
 
 def rel_errors(a, b):
+    """Per field, max |a-b| over the field's largest |b|; and for the height
+    h, which lift-off depends on near its minimum, the largest pointwise
+    |a-b|/|b| as well (h_pointwise)."""
     out = {}
     for k in FIELDS:
         den = max(np.max(np.abs(b[k])), 1e-300)
         out[k] = float(np.max(np.abs(np.asarray(a[k]) - np.asarray(b[k]))) / den)
+    hb = np.asarray(b["h"])
+    out["h_pointwise"] = float(np.max(np.abs(np.asarray(a["h"]) - hb) / np.abs(hb)))
     return out
 
 
