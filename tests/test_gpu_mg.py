@@ -309,3 +309,31 @@ def test_mac_neumann_config2_size(V):
     assert float(torch.linalg.norm(r) / torch.linalg.norm(bp)) <= 1e-10 * (1 + 1e-6)
     assert abs(float(s.z.mean())) <= 1e-12 * float(s.z.abs().max())
     assert v <= 30, v
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_repeated_solves_replay_the_same_solve(V, prec):
+    """The second and later solves of the same arrays run from a captured
+    graph (one launch, one status read): the same kernels in the same order
+    as the first, host-driven solve, so the same iterate bit for bit and the
+    same V-cycle count; a changed tolerance and the V-cycle cap still
+    apply."""
+    torch = _torch()
+    m, n = 256, 128
+    dx = 1. / m
+    b = torch.from_numpy(gaussians_rhs(m, n, seed=13)).cuda()
+    s = V.MgsMac(m, n, dx, 1.5 * dx)
+    s.b.copy_(b)
+    runs = []
+    for _ in range(3):
+        s.z.zero_()
+        runs.append((s.solve_v_cycle(rtol=1e-10, precision=prec), s.z.clone()))
+    for (v, _), z in runs[1:]:
+        assert v[0] == runs[0][0][0]
+        assert torch.equal(z, runs[0][1])
+    s.z.zero_()
+    v8, rel8 = s.solve_v_cycle(rtol=1e-8, precision=prec)
+    assert rel8 <= 1e-8 and v8 < runs[0][0][0]
+    s.z.zero_()
+    with pytest.raises(V.VdiError):
+        s.solve_v_cycle(rtol=1e-10, max_vcycles=1, precision=prec)

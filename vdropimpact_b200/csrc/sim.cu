@@ -984,7 +984,80 @@ int vdi_sim_vcycle_bytes(const vdi_sim* S, int precision, double* out4) {
 struct vdi_mg {
     MG* g = nullptr;
     cudaStream_t s = nullptr;
+    // solves replayed from a captured graph, per (b, z, precision): the
+    // start kernel and a conditional WHILE node over the V-cycles, so a
+    // solve is one launch and one read of the control block
+    struct Replay {
+        const double* b;
+        double* z;
+        int precision;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Replay> replays;
+    std::vector<std::pair<const double*, double*>> seen;   // solved once eagerly
+    cudaStream_t cap = nullptr;                             // capture stream
+    double rtol = -1;
+    int max_it = -1;
 };
+
+namespace {
+
+bool solve_graphs_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("VDI_MG_SOLVE_GRAPH");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+/** The solve of vdi_mg_solve from a captured graph (the second and later
+ * solves of the same arrays). */
+int mg_solve_replay(vdi_mg* h, const double* b, double* z, double rtol, int max_it, int precision, int* vcycles,
+                    double* rel_res) {
+    if (rtol != h->rtol || max_it != h->max_it) {
+        VDI_TRY(mg_configure(h->g, rtol, max_it));
+        h->rtol = rtol;
+        h->max_it = max_it;
+    }
+    cudaGraphExec_t exec = nullptr;
+    for (auto& r : h->replays)
+        if (r.b == b && r.z == z && r.precision == precision) exec = r.exec;
+    if (!exec) {
+        if (!h->cap) VDI_CUDA(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
+        VDI_CUDA(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+        int st = mg_record_graph_solve(h->g, h->cap, b, z, precision);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
+        if (st != VDI_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        VDI_CUDA(e);
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        VDI_CUDA(e);
+        h->replays.push_back(vdi_mg::Replay{b, z, precision, exec});
+    }
+    VDI_CUDA(cudaGraphLaunch(exec, h->s));
+    SolveCtl c;
+    VDI_CUDA(cudaMemcpyAsync(&c, mg_ctl(h->g), sizeof(SolveCtl), cudaMemcpyDeviceToHost, h->s));
+    VDI_CUDA(cudaStreamSynchronize(h->s));
+    if (vcycles) *vcycles = c.it;
+    if (rel_res) *rel_res = c.bnorm2 > 0 ? std::sqrt(c.rnorm2 / c.bnorm2) : 0.;
+    if (c.status & DEV_NONFINITE) {
+        set_error("multigrid: non-finite residual");
+        return VDI_ERR_NONFINITE;
+    }
+    if (c.status & DEV_MG_NOT_CONVERGED) {
+        set_error("multigrid: %d V-cycles without reaching rtol %.3g (rel. residual %.3g)", c.it, rtol,
+                  c.bnorm2 > 0 ? std::sqrt(c.rnorm2 / c.bnorm2) : 0.);
+        return VDI_ERR_MG_NOT_CONVERGED;
+    }
+    return VDI_OK;
+}
+
+}  // namespace
 
 int vdi_mg_create(int kind, int m, int n, double c1, double c2, int x_sym, void* stream, vdi_mg** out) {
     if (!out) return VDI_ERR_INVALID_ARGUMENT;
@@ -1007,6 +1080,8 @@ int vdi_mg_create(int kind, int m, int n, double c1, double c2, int x_sym, void*
 
 int vdi_mg_destroy(vdi_mg* h) {
     if (!h) return VDI_OK;
+    for (auto& r : h->replays) cudaGraphExecDestroy(r.exec);
+    if (h->cap) cudaStreamDestroy(h->cap);
     if (h->g) mg_destroy(h->g);
     delete h;
     return VDI_OK;
@@ -1019,7 +1094,19 @@ int vdi_mg_solve(vdi_mg* h, const double* d_b, double* d_z, double rtol, int max
     if (!h || !d_b || !d_z || !(rtol > 0) || max_vcycles < 0) return VDI_ERR_INVALID_ARGUMENT;
     int v = 0;
     double r = 0;
-    int st = mg_solve(h->g, h->s, d_b, d_z, rtol, max_vcycles, precision, &v, &r);
+    int st;
+    const std::pair<const double*, double*> key{d_b, d_z};
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (h->s) VDI_CUDA(cudaStreamIsCapturing(h->s, &cs));
+    const bool again = std::find(h->seen.begin(), h->seen.end(), key) != h->seen.end();
+    if (solve_graphs_enabled() && again && cs == cudaStreamCaptureStatusNone) {
+        st = mg_solve_replay(h, d_b, d_z, rtol, max_vcycles, precision, &v, &r);
+    } else {
+        st = mg_solve(h->g, h->s, d_b, d_z, rtol, max_vcycles, precision, &v, &r);
+        h->rtol = rtol;
+        h->max_it = max_vcycles;
+        if (!again && h->seen.size() < 64) h->seen.push_back(key);
+    }
     if (res) {
         res->vcycles = v;
         res->rel_res = r;
