@@ -368,6 +368,10 @@ int vdi_unet_create(int H, int W, int batch, unsigned seed, void* stream, vdi_un
 int vdi_unet_destroy(vdi_unet* net);
 long vdi_unet_param_count(const vdi_unet* net);
 int vdi_unet_forward(vdi_unet* net, const float* d_in, float* d_out, int batch);
+/* Which tensor-core path the convolutions take: 1 tcgen05.mma with TMEM
+ * accumulators, 0 mma.sync (the VDI_UNET_TC environment variable, read
+ * once per process, chooses). */
+int vdi_unet_tensor_path(void);
 /* One Adam step on the mean squared error of the output against d_target. */
 int vdi_unet_train_step(vdi_unet* net, const float* d_in, const float* d_target, int batch, float lr, float* h_loss);
 /* Loss and the weight gradient of one layer ([9][cout][cin], FP32) without

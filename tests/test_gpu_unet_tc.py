@@ -24,8 +24,8 @@ import json, sys
 import numpy as np
 import torch
 sys.path.insert(0, %r)
-from vdropimpact_b200 import learned
-out = {}
+from vdropimpact_b200 import learned, _abi
+out = {"path": _abi.lib().vdi_unet_tensor_path()}
 for (H, W) in ((32, 128), (24, 48), (64, 256)):
     net = learned.UNet(H, W, batch=2, seed=5)
     g = torch.Generator(device="cuda").manual_seed(H + W)
@@ -49,6 +49,7 @@ def run(tc: bool):
 
 def test_tensor_core_convolutions_match_mma_sync():
     a, b = run(False), run(True)
+    assert a.pop("path") == 0 and b.pop("path") == 1
     for key in a:
         for f in ("y", "g4", "g0"):
             x, y = np.array(a[key][f]), np.array(b[key][f])

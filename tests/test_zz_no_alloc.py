@@ -108,7 +108,10 @@ def test_noalloc_rejects_oversized_grid(L):
 def test_noalloc_near_the_size_limit(L, kind, m, n, c1, c2, x_sym):
     """The coarsest level is smoothed here and solved exactly by the
     allocating solve: both reach the residual tolerance and agree within the
-    tolerance the solves leave."""
+    tolerance the solves leave. On these larger grids, a 1e-10 residual
+    leaves errors of up to about 1e-9 of the solution's scale (the
+    anisotropic FEM grid more than the square MAC one), so two solves that
+    stop there are held to 1e-8 of each other."""
     for call, seed in enumerate((5, 6)):
         b = _gauss(m, n, seed)
         if kind == 1:
@@ -118,7 +121,9 @@ def test_noalloc_near_the_size_limit(L, kind, m, n, c1, c2, x_sym):
         za, va = _solve_allocating(L, kind, m, n, c1, c2, x_sym, b)
         zn, vn = _solve_noalloc(L, kind, m, n, c1, c2, x_sym, b)
         scale = max(np.abs(za).max(), 1e-300)
-        assert np.abs(zn - za).max() / scale <= TOL, (kind, call)
+        d = float(np.abs(zn - za).max() / scale)
+        print(f"no-alloc {kind} {m}x{n} call {call}: difference {d:.3e}, V-cycles {vn} vs {va}")
+        assert d <= 1e-8, (kind, call, d)
         assert abs(vn - va) <= 1, (kind, call, vn, va)
 
 

@@ -574,8 +574,8 @@ __device__ __forceinline__ T shfl_dn1(T v) { return __shfl_down_sync(0xffffffffu
 /** MODE 0: NS = 2 sweeps from zin (or zero), residual, restriction to bc
  * (skipped when bc is null). MODE 1: zin + prolonged zc, 2 sweeps, and
  * optionally the residual norm with the solve decision. Both write zout. */
-template <typename T, int MODE, typename TC = T>
-__global__ void __launch_bounds__(CCReg<T>::NT, 2) cc_rtile(CCc<T> c, TileArgs<T, TC> a) {
+template <typename T, int MODE, typename TC = T, int MINB = 2>
+__global__ void __launch_bounds__(CCReg<T>::NT, MINB) cc_rtile(CCc<T> c, TileArgs<T, TC> a) {
     using G = CCReg<T>;
     constexpr int R = G::R, CW = G::CW, CH = G::CH, K = G::K, ZH = G::ZH, NWARP = G::NWARP;
     __shared__ __align__(16) T edge[2][2][NWARP][CW];   // [buffer][first/last row][warp][column]
@@ -689,11 +689,15 @@ __global__ void __launch_bounds__(CCReg<T>::NT, 2) cc_rtile(CCc<T> c, TileArgs<T
             const T d = r > 0 ? z[r > 0 ? r - 1 : 0][h] : below[h];
             const T u = r < R - 1 ? z[r < R - 1 ? r + 1 : R - 1][h] : above[h];
             const int ii = 2 * lane + h, jj = warp * R + r;
-            if (ii < ph + 1 || ii > CW - 2 - ph || jj < ph + 1 || jj > CH - 2 - ph) continue;
-            if (!(unsigned(i) < unsigned(m) && unsigned(j) < unsigned(n))) continue;
+            // computed for every row and kept where the point is in the grid
+            // and exact in this phase: no branch between the (independent)
+            // rows, so their arithmetic interleaves
+            const bool upd = ii >= ph + 1 && ii <= CW - 2 - ph && jj >= ph + 1 && jj <= CH - 2 - ph &&
+                             unsigned(i) < unsigned(m) && unsigned(j) < unsigned(n);
             const T xs = (i > 0 ? l : T(0)) + (i < m - 1 ? rr : T(0));
             const T ys = (j > 0 ? d : T(0)) + (j < n - 1 ? u : T(0));
-            z[r][h] = (b[r][h] - (c.ox * xs + c.oy * ys)) * pick3(c.invd, cls(i, m), cls(j, n));
+            const T zn = (b[r][h] - (c.ox * xs + c.oy * ys)) * pick3(c.invd, cls(i, m), cls(j, n));
+            z[r][h] = upd ? zn : z[r][h];
         }
     }
     // interior back to global memory
@@ -987,8 +991,8 @@ struct FEMReg {
     static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
 };
 
-template <typename T, int MODE, typename TC = T>
-__global__ void __launch_bounds__(FEMReg<T>::NT, 2) fem_rtile(FEMc<T> c, TileArgs<T, TC> a) {
+template <typename T, int MODE, typename TC = T, int MINB = 2>
+__global__ void __launch_bounds__(FEMReg<T>::NT, MINB) fem_rtile(FEMc<T> c, TileArgs<T, TC> a) {
     using G = FEMReg<T>;
     constexpr int R = G::R, CW = G::CW, CH = G::CH, K = G::K, ZH = G::ZH, NWARP = G::NWARP;
     __shared__ __align__(16) T edge[2][2][NWARP][CW];
@@ -1079,10 +1083,11 @@ __global__ void __launch_bounds__(FEMReg<T>::NT, 2) fem_rtile(FEMc<T> c, TileArg
             const T dr = ci == 0 ? own[r] : nb[r];
             const T ul = ci == 0 ? nb[r + 2] : own[r + 2];
             const T ur = ci == 0 ? own[r + 2] : nb[r + 2];
-            if (ii < ph + 1 || ii > CW - 2 - ph || jj < ph + 1 || jj > CH - 2 - ph) continue;
-            if (!(unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N))) continue;
-            z[r][ci] = (b[r][ci] - fem_off_vals(c, i, j, dl, d, dr, l, rr, ul, u, ur)) *
-                       pick3(c.invd, cls(i, M), cls(j, N));
+            const bool upd = ii >= ph + 1 && ii <= CW - 2 - ph && jj >= ph + 1 && jj <= CH - 2 - ph &&
+                             unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N);
+            const T zn = (b[r][ci] - fem_off_vals(c, i, j, dl, d, dr, l, rr, ul, u, ur)) *
+                         pick3(c.invd, cls(i, M), cls(j, N));
+            z[r][ci] = upd ? zn : z[r][ci];
         }
     }
     const bool lanein = 2 * lane >= ZH && 2 * lane < ZH + G::TX;
@@ -1590,23 +1595,27 @@ struct LevelD {
     signed char gL, gR, gD, gU;
 };
 
-/** Which cell-centred tile kernel the V-cycles launch: the shared-memory
- * one (default) or the register-blocked one (VDI_MG_TILE=reg), read once. */
-static bool use_reg_tile() {
+/** Which tile kernels the V-cycles launch, read once: the shared-memory
+ * ones (0, default), or the register-blocked ones with two CTAs per SM
+ * (1, VDI_MG_TILE=reg) or one CTA per SM and its whole register file
+ * (2, VDI_MG_TILE=reg1). */
+static int reg_tile_mode() {
     static int v = -1;
     if (v < 0) {
         const char* e = getenv("VDI_MG_TILE");
-        v = (e && std::strcmp(e, "reg") == 0) ? 1 : 0;
+        v = !e ? 0 : (std::strcmp(e, "reg") == 0 ? 1 : (std::strcmp(e, "reg1") == 0 ? 2 : 0));
     }
-    return v == 1;
+    return v;
 }
+static bool use_reg_tile() { return reg_tile_mode() != 0; }
 
 template <typename T, int MODE, typename TC = T>
 static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T, TC>& a) {
     if (use_reg_tile()) {
         using G = CCReg<T>;
         dim3 grid((c.m + G::TX - 1) / G::TX, (c.n + G::TY - 1) / G::TY);
-        cc_rtile<T, MODE, TC><<<grid, G::NT, 0, s>>>(c, a);
+        if (reg_tile_mode() == 2) cc_rtile<T, MODE, TC, 1><<<grid, G::NT, 0, s>>>(c, a);
+        else cc_rtile<T, MODE, TC, 2><<<grid, G::NT, 0, s>>>(c, a);
         return;
     }
     using G = CCTile<T, 2>;
@@ -1619,7 +1628,8 @@ static void launch_fem_tile(cudaStream_t s, const FEMc<T>& c, const TileArgs<T, 
     if (use_reg_tile()) {
         using G = FEMReg<T>;
         dim3 grid((c.M + G::TX - 1) / G::TX, (c.N + G::TY - 1) / G::TY);
-        fem_rtile<T, MODE, TC><<<grid, G::NT, 0, s>>>(c, a);
+        if (reg_tile_mode() == 2) fem_rtile<T, MODE, TC, 1><<<grid, G::NT, 0, s>>>(c, a);
+        else fem_rtile<T, MODE, TC, 2><<<grid, G::NT, 0, s>>>(c, a);
         return;
     }
     using G = FEMTile<T>;

@@ -192,14 +192,17 @@ __global__ void __launch_bounds__(256) conv3x3_k(ConvArgs<TIN, TOUT> a) {
 // 16-byte core-matrix row, 8 consecutive pixels one 8 x 16-byte core
 // matrix, and the operand needs no copy per tap. The weights, already stored
 // [tap][cout][cin], are K-major B operands. A CTA stages the weights once and
-// then walks its row segments; each segment is 9 * CIN/16 MMAs (K = 16
-// each) into one accumulator, read back with tcgen05.ld for the bias,
-// skip-add, ReLU epilogue.
+// then walks a contiguous run of segments, consecutive rows of one segment
+// where it can, keeping the input rows in a ring of four: a new segment
+// stages one row, while the tensor cores work on the previous one. Each
+// segment is 9 * CIN/16 MMAs (K = 16 each) into one accumulator, read back
+// with tcgen05.ld for the bias, skip-add, ReLU epilogue.
 namespace tc {
 
 constexpr int TC_M = 128;            // output pixels per segment (MMA M)
 constexpr int TC_PX = TC_M + 2;      // staged pixels per input row (one halo pixel each side)
 constexpr int TC_THREADS = 128;
+constexpr int TC_RING = 4;           // staged input rows: three in use, the next being loaded
 
 __device__ int g_timeout;            // set when a bounded wait gave up
 
@@ -271,8 +274,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
-/** Dynamic shared memory of conv3x3_tc: the weights and three staged input
- * rows, plus TC_PAD bytes that no descriptor is meant to reach. The pad
+/** Dynamic shared memory of conv3x3_tc: the weights and the ring of staged
+ * input rows, plus TC_PAD bytes that no descriptor is meant to reach. The pad
  * keeps every address an operand could span inside the CTA's own
  * allocation even if the K and M core-matrix strides were interpreted the
  * other way round (the A operand would then reach 15 x 2080 + 128 bytes
@@ -281,7 +284,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 constexpr size_t TC_PAD = 32 * 1024;
 template <int CIN, int COUT>
 constexpr size_t tc_smem() {
-    return size_t(9) * (CIN / 8) * COUT * 16 + size_t(3) * (CIN / 8) * TC_PX * 16 + TC_PAD;
+    return size_t(9) * (CIN / 8) * COUT * 16 + size_t(TC_RING) * (CIN / 8) * TC_PX * 16 + TC_PAD;
 }
 
 template <int CIN, int COUT, typename TIN, typename TOUT>
@@ -294,7 +297,7 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc(ConvArgs<TIN, TOUT> a) 
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "tcgen05 shape");
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* wsm = smem;                               // [9][KC][COUT][8] bf16
-    unsigned char* rows = smem + 9 * WTAPB;                  // [3][KC][TC_PX][8] bf16
+    unsigned char* rows = smem + 9 * WTAPB;                  // ring [TC_RING][KC][TC_PX][8] bf16
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -320,22 +323,44 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc(ConvArgs<TIN, TOUT> a) 
     const uint32_t tmem = tmem_slot;
     constexpr uint32_t IDESC = idesc_bf16(TC_M, COUT);
     const int segs = (a.W + TC_M - 1) / TC_M;
+    // tasks in (segment, image, row) order; each CTA takes a contiguous run,
+    // so that consecutive tasks are usually consecutive rows of one segment
     const long tasks = long(a.B) * a.H * segs;
-    uint32_t phase = 0;
-    int ok = 1;
-    for (long task = blockIdx.x; task < tasks && ok; task += gridDim.x) {
-        const int seg = int(task % segs);
-        const long r = task / segs;
-        const int y = int(r % a.H), b = int(r / a.H), x0 = seg * TC_M;
-        // input rows y-1..y+1, pixels x0-1..x0+TC_M, as 16-byte channel chunks
-        for (int q = tid; q < 3 * KC * TC_PX; q += TC_THREADS) {
-            const int px = q % TC_PX, kc = (q / TC_PX) % KC, row = q / (TC_PX * KC);
-            const int yy = y + row - 1, xx = x0 + px - 1;
+    const long t0 = tasks * blockIdx.x / gridDim.x, t1 = tasks * (blockIdx.x + 1) / gridDim.x;
+    // input row yy of image b (pixels x0-1 .. x0+TC_M) into ring slot
+    // (yy + 1) % TC_RING, as 16-byte channel chunks
+    auto stage = [&](int b, int yy, int x0) {
+        unsigned char* dst = rows + uint32_t((yy + 1 + TC_RING) % TC_RING) * ROWB;
+        for (int q = tid; q < KC * TC_PX; q += TC_THREADS) {
+            const int px = q % TC_PX, kc = q / TC_PX;
+            const int xx = x0 + px - 1;
             uint4 v;
+            const bool in = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+            const size_t k8 = ((size_t(b) * a.H + yy) * a.W + xx) * CIN + kc * 8;
             if (std::is_same<TIN, bf16>::value && a.mode == SRC_DIRECT && !a.mask) {
-                const bool in = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
-                v = in ? *reinterpret_cast<const uint4*>(a.src + ((size_t(b) * a.H + yy) * a.W + xx) * CIN + kc * 8)
-                       : make_uint4(0, 0, 0, 0);
+                v = in ? *reinterpret_cast<const uint4*>(a.src + k8) : make_uint4(0, 0, 0, 0);
+            } else if (std::is_same<TIN, float>::value && a.mode == SRC_DIRECT) {
+                // FP32 source (the input gradient's dY), 8 channels in two
+                // 16-byte loads, the ReLU mask as one 16-byte load
+                __align__(16) bf16 e[8];
+                if (in) {
+                    const float4 lo = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(a.src) + k8);
+                    const float4 hi = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(a.src) + k8 + 4);
+                    float f[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+                    if (a.mask) {
+                        __align__(16) bf16 mk[8];
+                        *reinterpret_cast<uint4*>(mk) = *reinterpret_cast<const uint4*>(a.mask + k8);
+#pragma unroll
+                        for (int c = 0; c < 8; c++)
+                            if (!(__bfloat162float(mk[c]) > 0.f)) f[c] = 0.f;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 8; c++) e[c] = __float2bfloat16(f[c]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 8; c++) e[c] = __float2bfloat16(0.f);
+                }
+                v = *reinterpret_cast<const uint4*>(e);
             } else {
                 __align__(16) bf16 e[8];
 #pragma unroll
@@ -343,7 +368,20 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc(ConvArgs<TIN, TOUT> a) 
                     e[c] = __float2bfloat16(src_at(a.src, a.mask, a.mode, a.H, a.W, CIN, b, yy, xx, kc * 8 + c));
                 v = *reinterpret_cast<const uint4*>(e);
             }
-            *reinterpret_cast<uint4*>(rows + uint32_t(row) * ROWB + uint32_t(kc) * CHUNKB + uint32_t(px) * 16) = v;
+            *reinterpret_cast<uint4*>(dst + uint32_t(kc) * CHUNKB + uint32_t(px) * 16) = v;
+        }
+    };
+    uint32_t phase = 0;
+    int ok = 1;
+    int pseg = -1, pb = -1, py = -2;   // the previous task, whose next row is staged
+    for (long task = t0; task < t1 && ok; task++) {
+        const int y = int(task % a.H);
+        const long r = task / a.H;
+        const int b = int(r % a.B), seg = int(r / a.B), x0 = seg * TC_M;
+        if (!(seg == pseg && b == pb && y == py + 1)) {
+            stage(b, y - 1, x0);
+            stage(b, y, x0);
+            stage(b, y + 1, x0);
         }
         fence_async_smem();   // the staged rows (and weights) become visible to the tensor cores
         fence_before();
@@ -354,9 +392,10 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc(ConvArgs<TIN, TOUT> a) 
 #pragma unroll 1
             for (int t = 0; t < 9; t++) {
                 const int dy = t / 3, dx = t % 3;
+                unsigned char* src_row = rows + uint32_t((y + dy + TC_RING) % TC_RING) * ROWB;   // row y-1+dy
 #pragma unroll
                 for (int kb = 0; kb < CIN / 16; kb++) {
-                    const uint32_t aa = smem_u32(rows + uint32_t(dy) * ROWB + uint32_t(2 * kb) * CHUNKB + dx * 16);
+                    const uint32_t aa = smem_u32(src_row + uint32_t(2 * kb) * CHUNKB + dx * 16);
                     const uint32_t ba = smem_u32(wsm + uint32_t(t) * WTAPB + uint32_t(2 * kb) * COUT * 16);
                     mma_bf16_ss(tmem, sdesc(aa, CHUNKB, 128), sdesc(ba, uint32_t(COUT) * 16, 128), IDESC, acc);
                     acc = 1;
@@ -364,6 +403,12 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc(ConvArgs<TIN, TOUT> a) 
             }
             mma_commit(bar_a);
         }
+        // while the tensor cores run: the next task's new row, if it continues
+        // this segment, into the ring slot these MMAs do not read (row y-2's)
+        if (task + 1 < t1 && y + 1 < a.H) stage(b, y + 2, x0);
+        pseg = seg;
+        pb = b;
+        py = y;
         ok = mbar_wait(bar_a, phase) ? 1 : 0;
         phase ^= 1;
         ok = __syncthreads_and(ok);
@@ -871,6 +916,8 @@ static int tc_status(cudaStream_t s) {
     }
     return VDI_OK;
 }
+
+int vdi_unet_tensor_path(void) { return use_tc() ? 1 : 0; }
 
 int vdi_unet_forward(vdi_unet* u, const float* d_in, float* d_out, int batch) {
     if (!u || !d_in || !d_out || batch < 1 || batch > u->net->Bmax) return VDI_ERR_INVALID_ARGUMENT;
