@@ -328,12 +328,13 @@ def test_repeated_solves_replay_the_same_solve(V, prec):
     for _ in range(3):
         s.z.zero_()
         runs.append((s.solve_v_cycle(rtol=1e-10, precision=prec), s.z.clone()))
+    (v0, _), z0 = runs[0]
     for (v, _), z in runs[1:]:
-        assert v[0] == runs[0][0][0]
-        assert torch.equal(z, runs[0][1])
+        assert v == v0
+        assert torch.equal(z, z0)
     s.z.zero_()
     v8, rel8 = s.solve_v_cycle(rtol=1e-8, precision=prec)
-    assert rel8 <= 1e-8 and v8 < runs[0][0][0]
+    assert rel8 <= 1e-8 and v8 < v0
     s.z.zero_()
     with pytest.raises(V.VdiError):
         s.solve_v_cycle(rtol=1e-10, max_vcycles=1, precision=prec)

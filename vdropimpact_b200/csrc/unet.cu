@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(256) conv3x3_k(ConvArgs<TIN, TOUT> a) {
 }
 
 // ------------------------------------------- Blackwell tensor-core path
-// The same convolution on the fifth-generation tensor cores: tcgen05.mma with
+// The same convolution on the fifth-generation tensor cores (the default
+// path; VDI_UNET_TC=0 keeps the mma.sync kernel above): tcgen05.mma with
 // both operands in shared memory and the FP32 accumulator in tensor memory.
 // One CTA of four warps takes a row segment of TC_M = 128 output pixels
 // (the MMA's M), so the A operand of tap (dy, dx) is a window of the staged
@@ -663,12 +664,13 @@ struct Net {
     int step = 0;
 };
 
-/** Whether the convolutions run on tcgen05 (VDI_UNET_TC=1) or mma.sync. */
+/** Whether the forward and input-gradient convolutions run on tcgen05
+ * (default) or on mma.sync (VDI_UNET_TC=0), read once per process. */
 static bool use_tc() {
     static int v = -1;
     if (v < 0) {
         const char* e = getenv("VDI_UNET_TC");
-        v = (e && e[0] == '1') ? 1 : 0;
+        v = (e && e[0] == '0') ? 0 : 1;
     }
     return v == 1;
 }
