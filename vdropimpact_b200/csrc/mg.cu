@@ -26,6 +26,8 @@
 // inside FP64 iterative refinement use the same kernels with T = float.
 #include "vdi_internal.hh"
 
+#include <cudaTypedefs.h>
+
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -155,6 +157,9 @@ __device__ void solve_decide(SolveCtl* ctl, double r2, int count_cycle, int use_
             cont = 1;
         }
     }
+    // a failure recorded during the V-cycle (a tile kernel's copy that did
+    // not arrive) ends the solve too
+    if (ctl->status & (DEV_MG_NOT_CONVERGED | DEV_NONFINITE)) cont = 0;
     if (ctl->status) {
         ctl->sticky |= ctl->status;
         if (ctl->err_out) atomicOr(ctl->err_out, ctl->status);
@@ -574,45 +579,24 @@ __device__ __forceinline__ T shfl_dn1(T v) { return __shfl_down_sync(0xffffffffu
 /** MODE 0: NS = 2 sweeps from zin (or zero), residual, restriction to bc
  * (skipped when bc is null). MODE 1: zin + prolonged zc, 2 sweeps, and
  * optionally the residual norm with the solve decision. Both write zout. */
-template <typename T, int MODE, typename TC = T, int MINB = 2>
-__global__ void __launch_bounds__(CCReg<T>::NT, MINB) cc_rtile(CCc<T> c, TileArgs<T, TC> a) {
+/** One window of the register-blocked cell-centred tile (window origin zx,
+ * zy, both even) from z and b already in registers: the prolongation of the
+ * coarse correction (MODE 1), the colour phases, the interior written to
+ * zout and, when asked, the restriction to bc (MODE 0) or the thread's sum
+ * of squared residuals over the interior, returned (MODE 1 with norm). Every
+ * thread of the CTA must call it: the phases synchronise the CTA. */
+template <typename T, int MODE, typename TC>
+__device__ __forceinline__ double cc_rwin(const CCc<T>& c, const TileArgs<T, TC>& a, T (&z)[CCReg<T>::R][2],
+                                          const T (&b)[CCReg<T>::R][2], int zx, int zy,
+                                          T (*edge)[2][CCReg<T>::NWARP][CCReg<T>::CW]) {
     using G = CCReg<T>;
     constexpr int R = G::R, CW = G::CW, CH = G::CH, K = G::K, ZH = G::ZH, NWARP = G::NWARP;
-    __shared__ __align__(16) T edge[2][2][NWARP][CW];   // [buffer][first/last row][warp][column]
     const int m = c.m, n = c.n;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int zx = blockIdx.x * G::TX - ZH, zy = blockIdx.y * G::TY - ZH;
     const int i0 = zx + 2 * lane, j0 = zy + warp * R;
-    const bool read_z = MODE == 1 || !a.zero_init;
-    const bool vec = (m & 1) == 0 && ((reinterpret_cast<uintptr_t>(a.zin) | reinterpret_cast<uintptr_t>(a.b) |
-                                       reinterpret_cast<uintptr_t>(a.zout)) & (2 * sizeof(T) - 1)) == 0;
+    const bool vec = (m & 1) == 0 && (reinterpret_cast<uintptr_t>(a.zout) & (2 * sizeof(T) - 1)) == 0;
     using T2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
     const bool colin = i0 >= 0 && i0 + 1 < m;
-    T z[R][2], b[R][2];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        const int j = j0 + r;
-        const bool rowin = unsigned(j) < unsigned(n);
-        if (rowin && colin && vec) {
-            const long o = i0 + long(m) * j;
-            T2 bv = *reinterpret_cast<const T2*>(a.b + o);
-            b[r][0] = bv.x; b[r][1] = bv.y;
-            if (read_z) {
-                T2 zv = *reinterpret_cast<const T2*>(a.zin + o);
-                z[r][0] = zv.x; z[r][1] = zv.y;
-            } else {
-                z[r][0] = z[r][1] = T(0);
-            }
-        } else {
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int i = i0 + h;
-                const bool in = rowin && unsigned(i) < unsigned(m);
-                b[r][h] = in ? a.b[i + long(m) * j] : T(0);
-                z[r][h] = (in && read_z) ? a.zin[i + long(m) * j] : T(0);
-            }
-        }
-    }
     if constexpr (MODE == 1) {
         // prolongation: coarse cell I = i0/2 covers this thread's columns;
         // fine rows j0..j0+7 use coarse rows J0-1 .. J0+4
@@ -715,7 +699,7 @@ __global__ void __launch_bounds__(CCReg<T>::NT, MINB) cc_rtile(CCc<T> c, TileArg
         }
     }
     const bool want_resid = MODE == 0 ? a.bc != nullptr : a.norm != 0;
-    if (!want_resid) return;
+    if (!want_resid) return 0.;
     // residual of the final iterate at the thread's points (vertical
     // neighbours across warps once more through the shared array)
     {
@@ -758,6 +742,7 @@ __global__ void __launch_bounds__(CCReg<T>::NT, MINB) cc_rtile(CCc<T> c, TileArg
             const T s4 = res[2 * k][0] + res[2 * k][1] + res[2 * k + 1][0] + res[2 * k + 1][1];
             a.bc[I + long(mc) * J] = TC(T(0.25) * s4);
         }
+        return 0.;
     } else {
         double s = 0;
 #pragma unroll
@@ -771,9 +756,190 @@ __global__ void __launch_bounds__(CCReg<T>::NT, MINB) cc_rtile(CCc<T> c, TileArg
                 s += rv * rv;
             }
         }
-        s = block_sum(s);
+        return s;
+    }
+}
+
+/** The register-blocked tile as one window per CTA, loaded straight from
+ * global memory into registers. */
+template <typename T, int MODE, typename TC = T, int MINB = 2>
+__global__ void __launch_bounds__(CCReg<T>::NT, MINB) cc_rtile(CCc<T> c, TileArgs<T, TC> a) {
+    using G = CCReg<T>;
+    constexpr int R = G::R, CW = G::CW, ZH = G::ZH, NWARP = G::NWARP;
+    const int m = c.m, n = c.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int zx = blockIdx.x * G::TX - ZH, zy = blockIdx.y * G::TY - ZH;
+    const int i0 = zx + 2 * lane, j0 = zy + warp * R;
+    const bool read_z = MODE == 1 || !a.zero_init;
+    const bool vec = (m & 1) == 0 && ((reinterpret_cast<uintptr_t>(a.zin) | reinterpret_cast<uintptr_t>(a.b) |
+                                       reinterpret_cast<uintptr_t>(a.zout)) & (2 * sizeof(T) - 1)) == 0;
+    using T2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    const bool colin = i0 >= 0 && i0 + 1 < m;
+    T z[R][2], b[R][2];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int j = j0 + r;
+        const bool rowin = unsigned(j) < unsigned(n);
+        if (rowin && colin && vec) {
+            const long o = i0 + long(m) * j;
+            T2 bv = *reinterpret_cast<const T2*>(a.b + o);
+            b[r][0] = bv.x; b[r][1] = bv.y;
+            if (read_z) {
+                T2 zv = *reinterpret_cast<const T2*>(a.zin + o);
+                z[r][0] = zv.x; z[r][1] = zv.y;
+            } else {
+                z[r][0] = z[r][1] = T(0);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int i = i0 + h;
+                const bool in = rowin && unsigned(i) < unsigned(m);
+                b[r][h] = in ? a.b[i + long(m) * j] : T(0);
+                z[r][h] = (in && read_z) ? a.zin[i + long(m) * j] : T(0);
+            }
+        }
+    }
+    __shared__ __align__(16) T edge_s[2][2][NWARP][CW];
+    const double s = cc_rwin<T, MODE, TC>(c, a, z, b, zx, zy, edge_s);
+    if (MODE == 1 && a.norm) {
+        const double t = block_sum(s);
         double total;
-        if (grid_sum(s, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
+        if (grid_sum(t, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
+    }
+}
+
+// --------------------------------- persistent, TMA-fed register tile
+// The register-blocked window computation in a persistent kernel: one CTA
+// per SM walks windows blockIdx.x, blockIdx.x + gridDim.x, ..., and while it
+// computes one window, a bulk tensor copy (TMA, plain 2D loads of this GPU's
+// own arrays, no multicast) brings the next window's z and b into the other
+// half of a two-stage shared-memory ring. Threads take their 2 x 8 blocks from
+// the staged window, so the phases run from registers as in cc_rtile.
+// FP64 only: a window origin is even, and the copy's x coordinate must be a
+// multiple of 16 bytes.
+struct PTileStage {
+    static constexpr int W = CCReg<double>::CW, H = CCReg<double>::CH;
+    static constexpr size_t BYTES = size_t(W) * H * sizeof(double);   // one array of one window
+    static constexpr size_t SMEM = 4 * BYTES;                          // z and b, two stages
+};
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        :
+        : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))), "l"(map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+/** Bounded wait on an mbarrier phase (about 0.5 s of SM clock); false if it
+ * gave up. */
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > 1000000000LL) return false;
+    }
+}
+
+template <int MODE, typename TC>
+__global__ void __launch_bounds__(CCReg<double>::NT, 1)
+    cc_ptile(CCc<double> c, TileArgs<double, TC> a, const __grid_constant__ CUtensorMap mz,
+             const __grid_constant__ CUtensorMap mb, int nwx, int nwin) {
+    using G = CCReg<double>;
+    constexpr int R = G::R, CW = G::CW, ZH = G::ZH, NWARP = G::NWARP;
+    extern __shared__ __align__(1024) unsigned char sm_raw[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(16) double edge_s[2][2][NWARP][CW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool read_z = MODE == 1 || !a.zero_init;
+    const uint32_t tx = uint32_t(read_z ? 2 : 1) * uint32_t(PTileStage::BYTES);
+    auto zst = [&](int st) { return reinterpret_cast<double*>(sm_raw + size_t(2 * st) * PTileStage::BYTES); };
+    auto bst = [&](int st) { return reinterpret_cast<double*>(sm_raw + size_t(2 * st + 1) * PTileStage::BYTES); };
+    auto bar_of = [&](int st) { return static_cast<uint32_t>(__cvta_generic_to_shared(&bars[st])); };
+    auto issue = [&](int w, int st) {
+        const int zx = (w % nwx) * G::TX - ZH, zy = (w / nwx) * G::TY - ZH;
+        mbar_expect(bar_of(st), tx);
+        tma_load_2d(bst(st), &mb, zx, zy, bar_of(st));
+        if (read_z) tma_load_2d(zst(st), &mz, zx, zy, bar_of(st));
+    };
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < 2; st++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_of(st)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (int(blockIdx.x) < nwin) issue(blockIdx.x, 0);
+        if (int(blockIdx.x + gridDim.x) < nwin) issue(blockIdx.x + gridDim.x, 1);
+    }
+    double s = 0;
+    int ok = 1;
+    int k = 0;
+    int w = blockIdx.x;
+    for (; w < nwin; w += gridDim.x, k++) {
+        const int st = k & 1;
+        ok = mbar_wait_bounded(bar_of(st), uint32_t((k >> 1) & 1)) ? 1 : 0;
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
+        const int zx = (w % nwx) * G::TX - ZH, zy = (w / nwx) * G::TY - ZH;
+        double z[R][2], b[R][2];
+        const double* zs = zst(st);
+        const double* bs = bst(st);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int o = (warp * R + r) * CW + 2 * lane;
+            const double2 bv = *reinterpret_cast<const double2*>(bs + o);
+            b[r][0] = bv.x;
+            b[r][1] = bv.y;
+            if (read_z) {
+                const double2 zv = *reinterpret_cast<const double2*>(zs + o);
+                z[r][0] = zv.x;
+                z[r][1] = zv.y;
+            } else {
+                z[r][0] = z[r][1] = 0.;
+            }
+        }
+        // every thread has its values: the stage takes the window after next
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0 && w + 2 * int(gridDim.x) < nwin) issue(w + 2 * gridDim.x, st);
+        s += cc_rwin<double, MODE, TC>(c, a, z, b, zx, zy, edge_s);
+    }
+    if (!ok) {
+        // a copy did not arrive in time: the solve fails (its control block
+        // says so, and the owner's error word when there is one), and the
+        // copies that may still be in flight, windows k and k+1, get a
+        // bounded wait before the CTA leaves
+        if (threadIdx.x == 0) {
+            atomicOr(&a.ctl->status, int(DEV_MG_NOT_CONVERGED));
+            atomicOr(&a.ctl->sticky, int(DEV_MG_NOT_CONVERGED));
+            atomicExch(&a.ctl->tma_timeout, 1);
+            if (a.ctl->err_out) atomicOr(a.ctl->err_out, int(DEV_MG_NOT_CONVERGED));
+            for (int d = 0; d < 2; d++) {
+                const int kk = k + d;
+                if (w + d * int(gridDim.x) < nwin) (void)mbar_wait_bounded(bar_of(kk & 1), uint32_t((kk >> 1) & 1));
+            }
+        }
+        __syncthreads();
+        // the CTA still joins the norm's grid reduction below, so the solve's
+        // decision is made (and, with the failure bit set, ends the solve)
+    }
+    if (MODE == 1 && a.norm) {
+        const double t = block_sum(s);
+        double total;
+        if (grid_sum(t, a.rd, &total) && threadIdx.x == 0) solve_decide(a.ctl, total, 1, a.use_cond, a.h);
     }
 }
 
@@ -1596,21 +1762,133 @@ struct LevelD {
 };
 
 /** Which tile kernels the V-cycles launch, read once: the shared-memory
- * ones (0, default), or the register-blocked ones with two CTAs per SM
+ * ones (0, default), the register-blocked ones with two CTAs per SM
  * (1, VDI_MG_TILE=reg) or one CTA per SM and its whole register file
- * (2, VDI_MG_TILE=reg1). */
+ * (2, VDI_MG_TILE=reg1), or for FP64 cell-centred levels the persistent
+ * TMA-fed register tile (3, VDI_MG_TILE=tma; other levels as in 0). */
 static int reg_tile_mode() {
     static int v = -1;
     if (v < 0) {
         const char* e = getenv("VDI_MG_TILE");
-        v = !e ? 0 : (std::strcmp(e, "reg") == 0 ? 1 : (std::strcmp(e, "reg1") == 0 ? 2 : 0));
+        v = !e ? 0
+               : (std::strcmp(e, "reg") == 0 ? 1
+                  : (std::strcmp(e, "reg1") == 0 ? 2 : (std::strcmp(e, "tma") == 0 ? 3 : 0)));
     }
     return v;
 }
-static bool use_reg_tile() { return reg_tile_mode() != 0; }
+static bool use_reg_tile() { const int v = reg_tile_mode(); return v == 1 || v == 2; }
+
+/** The driver's tensor-map encoder, looked up once through the runtime so
+ * the library does not link libcuda itself; null when unavailable. */
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        else
+            cudaGetLastError();
+    }
+    return encode;
+}
+
+/** A 2D tensor map of an m x n FP64 array (row pitch m) with 64 x 64 boxes,
+ * zero fill outside the array: one per array, cached. False when the array
+ * cannot be described (odd m, unaligned base). */
+static bool tile_tensor_map(const double* p, int m, int n, CUtensorMap* out) {
+    if ((m & 1) || (reinterpret_cast<uintptr_t>(p) & 15)) return false;
+    struct Entry {
+        const double* p;
+        int m, n;
+        CUtensorMap map;
+    };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto& e : cache)
+        if (e.p == p && e.m == m && e.n == n) {
+            *out = e.map;
+            return true;
+        }
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return false;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {cuuint64_t(m), cuuint64_t(n)};
+    const cuuint64_t strides[1] = {cuuint64_t(m) * sizeof(double)};
+    const cuuint32_t box[2] = {uint32_t(PTileStage::W), uint32_t(PTileStage::H)};
+    const cuuint32_t es[2] = {1, 1};
+    CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(p), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    if (cache.size() >= 256) cache.erase(cache.begin());
+    cache.push_back(Entry{p, m, n, map});
+    *out = map;
+    return true;
+}
+
+/** The persistent tile's shared-memory opt-in, set once per instantiation. */
+template <int MODE, typename TC>
+static bool ptile_attr() {
+    static int state = -1;
+    if (state < 0) {
+        state = cudaFuncSetAttribute(cc_ptile<MODE, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(PTileStage::SMEM)) == cudaSuccess;
+        if (!state) cudaGetLastError();
+    }
+    return state == 1;
+}
+
+/** The one-time setup of the persistent tile, done when a hierarchy is
+ * created so that no lookup happens while a solve is being captured. */
+static void ptile_prepare() {
+    (void)tensor_map_encoder();
+    (void)ptile_attr<0, double>();
+    (void)ptile_attr<1, double>();
+    (void)ptile_attr<0, float>();
+    (void)ptile_attr<1, float>();
+}
+
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            n = 148;
+    }
+    return n;
+}
+
+/** The persistent TMA-fed tile for an FP64 cell-centred level; false when it
+ * does not apply (the caller then launches another tile kernel). */
+template <int MODE, typename TC>
+static bool launch_cc_ptile(cudaStream_t s, const CCc<double>& c, const TileArgs<double, TC>& a) {
+    CUtensorMap mz, mb;
+    const bool read_z = MODE == 1 || !a.zero_init;
+    if (!tile_tensor_map(a.b, c.m, c.n, &mb)) return false;
+    if (read_z) {
+        if (!tile_tensor_map(a.zin, c.m, c.n, &mz)) return false;
+    } else {
+        mz = mb;   // not read
+    }
+    if (!ptile_attr<MODE, TC>()) return false;
+    using G = CCReg<double>;
+    const int nwx = (c.m + G::TX - 1) / G::TX, nwy = (c.n + G::TY - 1) / G::TY, nwin = nwx * nwy;
+    const int grid = std::min(nwin, sm_count());
+    cc_ptile<MODE, TC><<<grid, G::NT, PTileStage::SMEM, s>>>(c, a, mz, mb, nwx, nwin);
+    return true;
+}
 
 template <typename T, int MODE, typename TC = T>
 static void launch_cc_tile(cudaStream_t s, const CCc<T>& c, const TileArgs<T, TC>& a) {
+    if constexpr (std::is_same<T, double>::value) {
+        if (reg_tile_mode() == 3 && launch_cc_ptile<MODE, TC>(s, c, a)) return;
+    }
     if (use_reg_tile()) {
         using G = CCReg<T>;
         dim3 grid((c.m + G::TX - 1) / G::TX, (c.n + G::TY - 1) / G::TY);
@@ -2346,6 +2624,7 @@ int mg_create(int kind, int m, int n, double c1, double c2, int x_sym, MG** out)
     }
     MG* g = new MG();
     g->kind = kind; g->m = m; g->n = n; g->c1 = c1; g->c2 = c2; g->x_sym = x_sym;
+    if (reg_tile_mode() == 3) ptile_prepare();
     int st = g->build_levels();
     if (st == VDI_OK) st = g->alloc();
     if (st != VDI_OK) {

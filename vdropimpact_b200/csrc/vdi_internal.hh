@@ -55,6 +55,7 @@ struct SolveCtl {
     double last_rel;
     int sticky;         // DevErr bits of every solve since creation
     int* err_out;       // when set, a failing solve also ORs its bits here
+    int tma_timeout;    // set when a tile kernel's bulk copy did not arrive in time
 };
 
 /** Deterministic block-then-grid sum: each block writes one partial, the
