@@ -192,6 +192,21 @@ struct FEMc {
 
 __device__ __forceinline__ int cls(int i, int m) { return i == 0 ? 0 : (i == m - 1 ? 2 : 1); }
 
+/** a[x][y] of a kernel-parameter table. FP32 selects the entry explicitly:
+ * indexing the parameter array with computed indices would copy it to the
+ * stack; FP64 indexes it (the selections would cost registers it lacks). */
+template <typename T>
+__device__ __forceinline__ T pick3(const T (&a)[3][3], int x, int y) {
+    if constexpr (sizeof(T) == 8) {
+        return a[x][y];
+    } else {
+        const T r0 = y == 0 ? a[0][0] : (y == 1 ? a[0][1] : a[0][2]);
+        const T r1 = y == 0 ? a[1][0] : (y == 1 ? a[1][1] : a[1][2]);
+        const T r2 = y == 0 ? a[2][0] : (y == 1 ? a[2][1] : a[2][2]);
+        return x == 0 ? r0 : (x == 1 ? r1 : r2);
+    }
+}
+
 /** Off-diagonal part of A z at (i,j); w points at z(i,j) in an array of
  * row pitch P. Neighbours outside the grid do not contribute, as in mul_a
  * of mgs_mac.hh:39-45 and visco_impl.hh:40-46. */
@@ -233,11 +248,11 @@ __device__ __forceinline__ int op_n(const FEMc<T>& c) { return c.N; }
 
 template <class OP, typename T>
 __device__ __forceinline__ T op_resid(const OP& c, const T* w, T bv, int P, int i, int j) {
-    return bv - c.d[cls(i, op_m(c))][cls(j, op_n(c))] * (*w) - op_off(c, w, P, i, j);
+    return bv - pick3(c.d, cls(i, op_m(c)), cls(j, op_n(c))) * (*w) - op_off(c, w, P, i, j);
 }
 template <class OP, typename T>
 __device__ __forceinline__ T op_relaxed(const OP& c, const T* w, T bv, int P, int i, int j) {
-    return (bv - op_off(c, w, P, i, j)) * c.invd[cls(i, op_m(c))][cls(j, op_n(c))];
+    return (bv - op_off(c, w, P, i, j)) * pick3(c.invd, cls(i, op_m(c)), cls(j, op_n(c)));
 }
 
 /** Bilinear cell-centred prolongation of the coarse correction to fine cell
@@ -300,8 +315,10 @@ __device__ __forceinline__ T fem_interp(const FEMc<T>& f, const TC* zc, int i, i
 
 /** P^T r at coarse node (I,J) from a residual array with origin (ox,oy) and
  * pitch P; zero on the Dirichlet bottom row. */
-template <typename T>
-__device__ __forceinline__ T fem_restrict_at(int M, int N, const T* r, int P, int ox, int oy, int I, int J) {
+/** P^T of the bilinear prolongation at coarse node (I, J), fine residuals
+ * read through at(i, j). */
+template <typename T, typename F>
+__device__ __forceinline__ T fem_restrict_by(int M, int N, F at, int I, int J) {
     if (J == 0) return T(0);
     T s = 0;
     for (int dj = -1; dj <= 1; dj++) {
@@ -312,10 +329,15 @@ __device__ __forceinline__ T fem_restrict_at(int M, int N, const T* r, int P, in
             int i = 2 * I + di;
             if (i < 0 || i >= M) continue;
             T wx = di == 0 ? T(1) : T(0.5);
-            s += wx * wy * r[(i - ox) + P * (j - oy)];
+            s += wx * wy * at(i, j);
         }
     }
     return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T fem_restrict_at(int M, int N, const T* r, int P, int ox, int oy, int I, int J) {
+    return fem_restrict_by<T>(M, N, [&](int i, int j) { return r[(i - ox) + P * (j - oy)]; }, I, J);
 }
 
 // ------------------------------------------------------- fused tile kernels
@@ -383,7 +405,7 @@ __device__ __forceinline__ void cc_window_phases(const CCc<T>& c, T* Z, const T*
                 if (unsigned(i) >= unsigned(m) || unsigned(j) >= unsigned(n)) continue;
                 T xs = (i > 0 ? l : T(0)) + (i < m - 1 ? r : T(0));
                 T ys = (j > 0 ? d : T(0)) + (j < n - 1 ? u : T(0));
-                *w = (Bc[jj * KW + lane] - (c.ox * xs + c.oy * ys)) * c.invd[cls(i, m)][cls(j, n)];
+                *w = (Bc[jj * KW + lane] - (c.ox * xs + c.oy * ys)) * pick3(c.invd, cls(i, m), cls(j, n));
             }
         }
         __syncthreads();
@@ -407,7 +429,7 @@ __device__ __forceinline__ double cc_window_epilogue(const CCc<T>& c, const Tile
         T bv = B[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)];
         T xs = (i > 0 ? zat(ii - 1, jj) : T(0)) + (i < m - 1 ? zat(ii + 1, jj) : T(0));
         T ys = (j > 0 ? zat(ii, jj - 1) : T(0)) + (j < n - 1 ? zat(ii, jj + 1) : T(0));
-        return bv - c.d[cls(i, m)][cls(j, n)] * zat(ii, jj) - (c.ox * xs + c.oy * ys);
+        return bv - pick3(c.d, cls(i, m), cls(j, n)) * zat(ii, jj) - (c.ox * xs + c.oy * ys);
     };
     // interior back to global memory (coalesced by row)
     for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
@@ -435,12 +457,16 @@ __device__ __forceinline__ double cc_window_epilogue(const CCc<T>& c, const Tile
             }
         }
     } else if (a.norm) {
+        // a warp takes the row's cells of one colour (every other column),
+        // so each read of the residual is consecutive words of one colour
+        // array; consecutive columns alternate arrays whose words share banks
+        static_assert(TX / 2 <= 32 && TX % 2 == 0, "one warp per colour row");
         for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
             const int j = zy + jj;
             if (j >= n) break;
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int ii = ZH + lane + 32 * h;
+            for (int ci = 0; ci < 2; ci++) {
+                const int ii = ZH + ci + 2 * lane;
                 if (ii < ZH + TX && zx + ii < m) {
                     double r = double(resid(ii, jj));
                     s += r * r;
@@ -556,20 +582,6 @@ struct CCReg {
     static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
 };
 
-/** a[x][y] of a kernel-parameter table. FP32 selects the entry explicitly:
- * indexing the parameter array with computed indices would copy it to the
- * stack; FP64 indexes it (the selections would cost registers it lacks). */
-template <typename T>
-__device__ __forceinline__ T pick3(const T (&a)[3][3], int x, int y) {
-    if constexpr (sizeof(T) == 8) {
-        return a[x][y];
-    } else {
-        const T r0 = y == 0 ? a[0][0] : (y == 1 ? a[0][1] : a[0][2]);
-        const T r1 = y == 0 ? a[1][0] : (y == 1 ? a[1][1] : a[1][2]);
-        const T r2 = y == 0 ? a[2][0] : (y == 1 ? a[2][1] : a[2][2]);
-        return x == 0 ? r0 : (x == 1 ? r1 : r2);
-    }
-}
 
 template <typename T>
 __device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
@@ -1077,7 +1089,7 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
                 const int i = zx + ii, j = zy + jj;
                 if (unsigned(i) >= unsigned(M) || unsigned(j) >= unsigned(N)) continue;
                 *w = (Bc[jr * QW + ir] - fem_off_vals(c, i, j, dl, d, dr, l, r, ul, u, ur)) *
-                     c.invd[cls(i, M)][cls(j, N)];
+                     pick3(c.invd, cls(i, M), cls(j, N));
             }
         }
         __syncthreads();
@@ -1087,7 +1099,7 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
         const int i = zx + ii, j = zy + jj;
         T off = fem_off_vals(c, i, j, zat(ii - 1, jj - 1), zat(ii, jj - 1), zat(ii + 1, jj - 1), zat(ii - 1, jj),
                              zat(ii + 1, jj), zat(ii - 1, jj + 1), zat(ii, jj + 1), zat(ii + 1, jj + 1));
-        return B[qidx(ii, jj)] - c.d[cls(i, M)][cls(j, N)] * zat(ii, jj) - off;
+        return B[qidx(ii, jj)] - pick3(c.d, cls(i, M), cls(j, N)) * zat(ii, jj) - off;
     };
     for (int jj = ZH + warp; jj < ZH + TY; jj += NW) {
         const int j = zy + jj;
@@ -1099,13 +1111,28 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
             if (ii < ZH + TX && i < M) a.zout[i + M * j] = zat(ii, jj);
         }
     }
+    // The residual passes give a warp 32 points of one column parity, so
+    // each of the residual's reads is 32 consecutive words of one quarter
+    // (consecutive window columns alternate quarters: a warp over them
+    // would read two quarters' words in the same banks).
+    static_assert(ZH % 2 == 0 && (RW + 1) / 2 <= 32 && TX / 2 <= 32, "one warp per colour row");
     if (MODE == 0) {
-        // residuals on the interior and one ring, then P^T onto coarse nodes
+        // residuals on the interior and one ring, held as four colour
+        // quarters (ring column/row ZH-1+2k and ZH+2k share index k), then
+        // P^T onto coarse nodes
+        constexpr int RQ = (RW + 1) / 2, RQN = RQ * ((RH + 1) / 2);
+        static_assert(4 * RQN <= RW * RH, "ring quarters fit the ring array");
+        auto ridx = [](int ii, int jj) {
+            return ((ii & 1) + 2 * (jj & 1)) * RQN + ((jj - (ZH - 1)) >> 1) * RQ + ((ii - (ZH - 1)) >> 1);
+        };
         for (int jr = warp; jr < RH; jr += NW) {
             const int jj = ZH - 1 + jr, j = zy + jj;
-            for (int ir = lane; ir < RW; ir += 32) {
-                const int ii = ZH - 1 + ir, i = zx + ii;
-                R[jr * RW + ir] = (unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N)) ? resid(ii, jj) : T(0);
+#pragma unroll
+            for (int ci = 0; ci < 2; ci++) {
+                const int ii = ZH - 1 + (1 - ci) + 2 * lane;   // ZH - 1 is odd
+                if (ii >= ZH - 1 + RW) continue;
+                const int i = zx + ii;
+                R[ridx(ii, jj)] = (unsigned(i) < unsigned(M) && unsigned(j) < unsigned(N)) ? resid(ii, jj) : T(0);
             }
         }
         __syncthreads();
@@ -1115,7 +1142,7 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
             const int q = t / CX;
             const int I = x0 / 2 + (t - q * CX), J = y0 / 2 + q;
             if (I >= Mc || J >= Nc) continue;
-            a.bc[I + Mc * J] = TC(fem_restrict_at(M, N, R, RW, x0 - 1, y0 - 1, I, J));
+            a.bc[I + Mc * J] = TC(fem_restrict_by<T>(M, N, [&](int i, int j) { return R[ridx(i - zx, j - zy)]; }, I, J));
         }
     } else if (a.norm) {
         double s = 0;
@@ -1123,8 +1150,8 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
             const int j = zy + jj;
             if (j >= N) break;
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int ii = ZH + lane + 32 * h;
+            for (int ci = 0; ci < 2; ci++) {
+                const int ii = ZH + ci + 2 * lane;
                 if (ii < ZH + TX && zx + ii < M) {
                     double r = double(resid(ii, jj));
                     s += r * r;
@@ -1695,7 +1722,7 @@ __global__ void apply_k(OP c, const T* __restrict__ z, T* __restrict__ y) {
     if (k >= tot) return;
     int i, j;
     grid_ij(c, k, i, j);
-    y[k] = c.d[cls(i, op_m(c))][cls(j, op_n(c))] * z[k] + op_off(c, z + k, op_m(c), i, j);
+    y[k] = pick3(c.d, cls(i, op_m(c)), cls(j, op_n(c))) * z[k] + op_off(c, z + k, op_m(c), i, j);
 }
 
 template <typename T, class OP>

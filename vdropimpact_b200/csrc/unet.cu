@@ -678,16 +678,25 @@ static bool use_tc() {
 template <int CIN, int COUT, typename TIN, typename TOUT>
 static cudaError_t conv_launch(cudaStream_t s, const ConvArgs<TIN, TOUT>& a) {
     if (use_tc()) {
-        static bool tattr = false;
-        if (!tattr) {
+        // one wave of resident CTAs: each takes a contiguous run of tasks and
+        // stages the next rows while its MMAs run
+        static int resident = 0;
+        if (!resident) {
             cudaError_t e = cudaFuncSetAttribute(tc::conv3x3_tc<CIN, COUT, TIN, TOUT>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  int(tc::tc_smem<CIN, COUT>()));
             if (e != cudaSuccess) return e;
-            tattr = true;
+            int dev = 0, sms = 0, per_sm = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+                (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+                (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::conv3x3_tc<CIN, COUT, TIN, TOUT>,
+                                                                   tc::TC_THREADS, tc::tc_smem<CIN, COUT>())) !=
+                    cudaSuccess)
+                return e;
+            resident = sms * (per_sm > 0 ? per_sm : 1);
         }
         const long tasks = long(a.B) * a.H * ((a.W + tc::TC_M - 1) / tc::TC_M);
-        const int grid = int(tasks < 296 ? tasks : 296);
+        const int grid = int(tasks < resident ? tasks : resident);
         tc::conv3x3_tc<CIN, COUT, TIN, TOUT><<<grid, tc::TC_THREADS, tc::tc_smem<CIN, COUT>(), s>>>(a);
         return cudaGetLastError();
     }
