@@ -356,6 +356,13 @@ int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* 
  * 16: a thread-block cluster whose CTAs hold row slabs of every level). No
  * reference counterpart. */
 int vdi_mg_coarse_cycle(const vdi_mg* mg, int precision, int* first_level, int* ctas);
+/* Which kernel runs the tiled levels, read once per process from
+ * VDI_MG_TILE: 0 the shared-memory tiles (default), 1 register-blocked
+ * tiles at two CTAs per SM ("reg"), 2 the same at one CTA per SM ("reg1"),
+ * 3 the persistent TMA-fed register tile on FP64 cell-centred levels, the
+ * others as in 0 ("tma"). *persistent_launches (if not null) receives the
+ * persistent tile's launches issued so far, a captured graph's once. */
+int vdi_mg_tile_path(long long* persistent_launches);
 
 /* ------------------------------------------------------------ U-Net
  * The learned initial guess has no counterpart in the reference. A small

@@ -125,6 +125,7 @@ _SIGS = [
     ("vdi_sim_get_params", C.c_int, [C.c_void_p, C.POINTER(VdiParams)]),
     ("vdi_unet_guess", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     ("vdi_unet_tensor_path", C.c_int, []),
+    ("vdi_mg_tile_path", C.c_int, [C.POINTER(C.c_longlong)]),
     ("vdi_sim_init_tracers", C.c_int, [C.c_void_p]),
     ("vdi_sim_update_tracers", C.c_int, [C.c_void_p, C.c_double]),
     ("vdi_sim_set_nif_mode", C.c_int, [C.c_void_p, C.c_int, C.c_double]),

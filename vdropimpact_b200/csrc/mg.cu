@@ -31,6 +31,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
@@ -363,7 +364,11 @@ struct CCTile {
     static constexpr int K = 2 * NS, ZH = K + 1;
     static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
     static constexpr int NT = 512, NW = NT / 32;
-    static constexpr size_t smem = size_t(4) * CH * KW * sizeof(T);
+    // the two colour arrays of z (and of b) sit 64 bytes off each other's
+    // bank alignment: a warp over consecutive columns alternates between
+    // them, and its half-warps then fall in different banks
+    static constexpr int CSTR = CH * KW + 64 / int(sizeof(T));
+    static constexpr size_t smem = size_t(4) * CSTR * sizeof(T);
 };
 
 /** MODE 0: NS sweeps from zin (or zero), residual, restriction to bc (skipped
@@ -382,9 +387,9 @@ __device__ __forceinline__ void cc_window_phases(const CCc<T>& c, T* Z, const T*
 #pragma unroll
     for (int ph = 0; ph < K; ph++) {
         const int color = MODE == 1 ? ((ph & 1) ^ 1) : (ph & 1);
-        T* Zc = Z + color * CH * KW;
-        const T* Zo = Z + (color ^ 1) * CH * KW;
-        const T* Bc = B + color * CH * KW;
+        T* Zc = Z + color * G::CSTR;
+        const T* Zo = Z + (color ^ 1) * G::CSTR;
+        const T* Bc = B + color * G::CSTR;
 #pragma unroll
         for (int q = 0; q < RPW; q++) {
             const int jj = warp + q * NW;
@@ -423,10 +428,10 @@ __device__ __forceinline__ double cc_window_epilogue(const CCc<T>& c, const Tile
     constexpr int NW = G::NW;
     const int m = c.m, n = c.n;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    auto zat = [&](int ii, int jj) -> T { return Z[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)]; };
+    auto zat = [&](int ii, int jj) -> T { return Z[((par0 + ii + jj) & 1) * G::CSTR + jj * KW + (ii >> 1)]; };
     auto resid = [&](int ii, int jj) -> T {
         const int i = zx + ii, j = zy + jj;
-        T bv = B[((par0 + ii + jj) & 1) * CH * KW + jj * KW + (ii >> 1)];
+        T bv = B[((par0 + ii + jj) & 1) * G::CSTR + jj * KW + (ii >> 1)];
         T xs = (i > 0 ? zat(ii - 1, jj) : T(0)) + (i < m - 1 ? zat(ii + 1, jj) : T(0));
         T ys = (j > 0 ? zat(ii, jj - 1) : T(0)) + (j < n - 1 ? zat(ii, jj + 1) : T(0));
         return bv - pick3(c.d, cls(i, m), cls(j, n)) * zat(ii, jj) - (c.ox * xs + c.oy * ys);
@@ -484,7 +489,7 @@ __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<
     constexpr int NW = G::NW, RPW = CH / NW;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* Z = reinterpret_cast<T*>(sm_raw);
-    T* B = Z + 2 * CH * KW;
+    T* B = Z + 2 * G::CSTR;
     const int m = c.m, n = c.n;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int zx = x0 - ZH, zy = y0 - ZH;
@@ -544,8 +549,8 @@ __global__ void __launch_bounds__(CCTile<T, NS>::NT) cc_tile(CCc<T> c, TileArgs<
             for (int h = 0; h < 2; h++) {
                 int ii = lane + 32 * h;
                 int col = (par0 + ii + jj) & 1;
-                Z[col * CH * KW + jj * KW + (ii >> 1)] = zv[q][h];
-                B[col * CH * KW + jj * KW + (ii >> 1)] = bv[q][h];
+                Z[col * G::CSTR + jj * KW + (ii >> 1)] = zv[q][h];
+                B[col * G::CSTR + jj * KW + (ii >> 1)] = bv[q][h];
             }
         }
     }
@@ -970,7 +975,10 @@ struct FEMTile {
     static constexpr int TX = CW - 2 * ZH, TY = CH - 2 * ZH;
     static constexpr int RW = TX + 2, RH = TY + 2;
     static constexpr int NT = 512, NW = NT / 32;
-    static constexpr size_t smem = (size_t(8) * QN + size_t(RW) * RH) * sizeof(T);
+    // quarters 64 bytes off each other's bank alignment, for the passes in
+    // which a warp over consecutive columns alternates between two of them
+    static constexpr int QS = QN + 64 / int(sizeof(T));
+    static constexpr size_t smem = (size_t(8) * QS + size_t(RW) * RH) * sizeof(T);
 };
 
 /** mul_a of mgs_fem.cc:32-53 from neighbour values (dl d dr / l r / ul u ur). */
@@ -995,15 +1003,15 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
     constexpr int CH = G::CH, RW = G::RW, RH = G::RH;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* Z = reinterpret_cast<T*>(sm_raw);     // 4 quarters
-    T* B = Z + 4 * QN;                       // 4 quarters
-    T* R = B + 4 * QN;                       // residual ring array (PRE)
+    T* B = Z + 4 * G::QS;                    // 4 quarters
+    T* R = B + 4 * G::QS;                    // residual ring array (PRE)
     const int M = c.M, N = c.N;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int zx = x0 - ZH, zy = y0 - ZH;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool inner = zx >= 0 && zy >= 0 && zx + G::CW <= M && zy + CH <= N && zy > 0;
     const bool read_z = MODE == 1 || !a.zero_init;
-    auto qidx = [](int ii, int jj) { return ((ii & 1) + 2 * (jj & 1)) * QN + (jj >> 1) * QW + (ii >> 1); };
+    auto qidx = [](int ii, int jj) { return ((ii & 1) + 2 * (jj & 1)) * G::QS + (jj >> 1) * QW + (ii >> 1); };
     {
         constexpr int RPW = CH / NW;
         T zv[RPW][2], bv[RPW][2];
@@ -1065,11 +1073,11 @@ __global__ void __launch_bounds__(FEMTile<T>::NT) fem_tile(FEMc<T> c, TileArgs<T
     for (int ph = 0; ph < K; ph++) {
         const int color = MODE == 1 ? 3 - (ph & 3) : (ph & 3);
         const int ci = color & 1, cj = color >> 1;
-        T* Zc = Z + color * QN;
-        const T* Zx = Z + (color ^ 1) * QN;   // (1-ci, cj): left/right
-        const T* Zy = Z + (color ^ 2) * QN;   // (ci, 1-cj): down/up
-        const T* Zd = Z + (color ^ 3) * QN;   // (1-ci, 1-cj): diagonals
-        const T* Bc = B + color * QN;
+        T* Zc = Z + color * G::QS;
+        const T* Zx = Z + (color ^ 1) * G::QS;   // (1-ci, cj): left/right
+        const T* Zy = Z + (color ^ 2) * G::QS;   // (ci, 1-cj): down/up
+        const T* Zd = Z + (color ^ 3) * G::QS;   // (1-ci, 1-cj): diagonals
+        const T* Bc = B + color * G::QS;
 #pragma unroll
         for (int q = 0; q < QW / NW; q++) {
             const int jr = warp + q * NW, ir = lane;
@@ -1805,6 +1813,15 @@ static int reg_tile_mode() {
 }
 static bool use_reg_tile() { const int v = reg_tile_mode(); return v == 1 || v == 2; }
 
+/** Launches of the persistent tile issued so far (a captured graph's count
+ * once, at capture). */
+static std::atomic<long long> g_ptile_launches{0};
+
+int mg_tile_path(long long* persistent_launches) {
+    if (persistent_launches) *persistent_launches = g_ptile_launches.load(std::memory_order_relaxed);
+    return reg_tile_mode();
+}
+
 /** The driver's tensor-map encoder, looked up once through the runtime so
  * the library does not link libcuda itself; null when unavailable. */
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -1908,6 +1925,7 @@ static bool launch_cc_ptile(cudaStream_t s, const CCc<double>& c, const TileArgs
     const int nwx = (c.m + G::TX - 1) / G::TX, nwy = (c.n + G::TY - 1) / G::TY, nwin = nwx * nwy;
     const int grid = std::min(nwin, sm_count());
     cc_ptile<MODE, TC><<<grid, G::NT, PTileStage::SMEM, s>>>(c, a, mz, mb, nwx, nwin);
+    g_ptile_launches.fetch_add(1, std::memory_order_relaxed);
     return true;
 }
 

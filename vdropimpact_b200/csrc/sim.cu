@@ -1165,6 +1165,8 @@ int vdi_mg_coarse_cycle(const vdi_mg* h, int precision, int* first_level, int* c
     return mg_coarse_cycle(h->g, precision, first_level, ctas);
 }
 
+int vdi_mg_tile_path(long long* persistent_launches) { return mg_tile_path(persistent_launches); }
+
 int vdi_mg_profile(vdi_mg* h, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
                    double* bytes_per_launch) {
     if (!h || !d_b || !d_z || !ms_per_launch || !bytes_per_launch || which < 0 || which > 3)

@@ -125,6 +125,10 @@ int mg_configure(MG* mg, double rtol, int max_it);
 /** A device word that failing solves OR their DevErr bits into (the
  * owner's error word), kept across rebuilds of the hierarchy. */
 int mg_set_error_word(MG* mg, int* d_err);
+/* The finest-tile variant (0 shared memory, 1 and 2 register-blocked, 3
+ * persistent TMA-fed for FP64 cell-centred levels) and the persistent
+ * tile's launches so far. */
+int mg_tile_path(long long* persistent_launches);
 /** Builds the conditional-node loop for the solve into a graph under
  * stream capture. Returns VDI_OK when a graph loop was recorded. */
 int mg_record_graph_solve(MG* mg, cudaStream_t s, const double* b, double* z, int precision);
