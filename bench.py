@@ -256,9 +256,9 @@ def measured_peak_gbs():
 
 
 # DRAM bytes (read + write) of one launch of the roofline kernel, from an ncu
-# capture of the same kernel on a 4096x2048 grid (196.3 MB per launch),
+# capture of the same kernel on a 4096x2048 grid (192.3 MB per launch),
 # scaled to the 2048x1024 bench grid by the number of cells.
-CC_POST_DRAM_BYTES = 196.3e6 / 4
+CC_POST_DRAM_BYTES = 192.3e6 / 4
 
 
 def roofline(V, torch, args):

@@ -353,7 +353,9 @@ int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* 
 /* The coarse levels of a V-cycle (of the given vdi_mg_precision) that run in
  * one launch: the first such level (level 0 the finest; -1 when the
  * hierarchy has none) and the CTAs of that launch (1: a single CTA; 8 or
- * 16: a thread-block cluster whose CTAs hold row slabs of every level). No
+ * 16: a thread-block cluster whose CTAs hold row slabs of every level; 0:
+ * that level is solved exactly by a dense inverse applied over the whole
+ * GPU, as FEM hierarchies do when it has at most 3072 unknowns). No
  * reference counterpart. */
 int vdi_mg_coarse_cycle(const vdi_mg* mg, int precision, int* first_level, int* ctas);
 /* Which kernel runs the tiled levels, read once per process from

@@ -77,11 +77,56 @@ def test_cluster_solves_match_single_cta(V, m, n, top, cs, prec, monkeypatch):
     assert _rel(res[True][1], res[False][1]) < 1e-8
 
 
-def test_cluster_cycle_reports_single_cta_for_other_systems(V):
-    """The FEM, Neumann and viscous hierarchies keep their own coarse path."""
+def test_cluster_cycle_reports_single_cta_for_other_systems(V, monkeypatch):
+    """The FEM, Neumann and viscous hierarchies keep their own coarse path:
+    the FEM one solves its first CTA-sized level (65x33 here) exactly over
+    the whole GPU (0 CTAs), or runs the single-CTA cycle with
+    VDI_MG_FEM_DIRECT=0."""
     fem = V.MgsFem(129, 65, 1 / 128, 1 / 128)
-    assert fem.coarse_cycle()[1] == 1
+    assert fem.coarse_cycle() == (1, 0)
+    monkeypatch.setenv("VDI_MG_FEM_DIRECT", "0")
+    fem = V.MgsFem(129, 65, 1 / 128, 1 / 128)
+    monkeypatch.delenv("VDI_MG_FEM_DIRECT")
+    assert fem.coarse_cycle() == (1, 1)
     neu = V.MgsMacNeumann(256, 128, 1 / 256, 1 / 256)
     assert neu.coarse_cycle()[1] == 1
     visc = V.ViscoImpl(256, 128, True, True, 5., 5.)
     assert visc.coarse_cycle() == (-1, 0)
+
+
+# FEM grids whose first CTA-sized level (65x33, 2145 nodes) is solved
+# exactly over the whole GPU
+FEM_CASES = [(2049, 1025, 5), (1025, 513, 4), (257, 129, 2)]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "hybrid"])
+@pytest.mark.parametrize("M,N,first", FEM_CASES)
+def test_fem_direct_coarse_solve_matches_cta_cycle(V, M, N, first, prec, monkeypatch):
+    """The whole-GPU exact solve of the coarse FEM level against the
+    single-CTA cycle (smoothing down to the 256-node exact level): both
+    solves reach the 1e-10 residual and agree to its accuracy; the exact
+    coarse solve takes no more V-cycles."""
+    import torch
+    g = torch.Generator().manual_seed(M + N)
+    b = torch.randn(M * N, dtype=torch.float64, generator=g)
+    b[:M] = 0.3
+    res = {}
+    for direct in (True, False):
+        monkeypatch.setenv("VDI_MG_FEM_DIRECT", "1" if direct else "0")
+        s = V.MgsFem(M, N, 1.0 / (M - 1), 1.5 / (M - 1))
+        monkeypatch.delenv("VDI_MG_FEM_DIRECT")
+        f, ctas = s.coarse_cycle(precision=prec if prec == "mixed" else None)
+        if direct:
+            assert (f, ctas) == (first, 0)
+        else:
+            assert ctas == 1
+        s.b.copy_(b)
+        s.z.zero_()
+        v, rel = s.solve_v_cycle(rtol=1e-10, precision=prec)
+        assert rel <= 1e-10
+        r, nr = s.residual()
+        assert nr / float(b.norm()) <= 1e-10 * (1 + 1e-6)
+        res[direct] = (v, s.z.cpu().numpy().copy())
+        print(M, N, prec, "direct" if direct else "cta", v)
+    assert res[True][0] <= res[False][0]
+    assert _rel(res[True][1], res[False][1]) < 1e-8

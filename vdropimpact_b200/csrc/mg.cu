@@ -45,6 +45,10 @@ static constexpr int CTA_THREADS = 1024;
 static constexpr size_t CTA_SMEM_LIMIT = 200 * 1024;
 static constexpr int MAX_PARTIALS = 8192;
 static constexpr int DIRECT_MAX = 256;
+// A FEM hierarchy whose first CTA-resident level has more than DIRECT_MAX but
+// at most GDIRECT_MAX unknowns solves that level exactly with a dense
+// inverse applied by the whole GPU, in place of the single-CTA cycle.
+static constexpr int GDIRECT_MAX = 3072;   // a 75 MB FP64 inverse at most
 
 // ------------------------------------------------------------------ reduce
 __device__ __forceinline__ double warp_sum(double v) {
@@ -876,14 +880,14 @@ __global__ void __launch_bounds__(CCReg<double>::NT, 1)
              const __grid_constant__ CUtensorMap mb, int nwx, int nwin) {
     using G = CCReg<double>;
     constexpr int R = G::R, CW = G::CW, ZH = G::ZH, NWARP = G::NWARP;
-    extern __shared__ __align__(1024) unsigned char sm_raw[];
+    extern __shared__ __align__(1024) unsigned char pt_raw[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ __align__(16) double edge_s[2][2][NWARP][CW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool read_z = MODE == 1 || !a.zero_init;
     const uint32_t tx = uint32_t(read_z ? 2 : 1) * uint32_t(PTileStage::BYTES);
-    auto zst = [&](int st) { return reinterpret_cast<double*>(sm_raw + size_t(2 * st) * PTileStage::BYTES); };
-    auto bst = [&](int st) { return reinterpret_cast<double*>(sm_raw + size_t(2 * st + 1) * PTileStage::BYTES); };
+    auto zst = [&](int st) { return reinterpret_cast<double*>(pt_raw + size_t(2 * st) * PTileStage::BYTES); };
+    auto bst = [&](int st) { return reinterpret_cast<double*>(pt_raw + size_t(2 * st + 1) * PTileStage::BYTES); };
     auto bar_of = [&](int st) { return static_cast<uint32_t>(__cvta_generic_to_shared(&bars[st])); };
     auto issue = [&](int w, int st) {
         const int zx = (w % nwx) * G::TX - ZH, zy = (w / nwx) * G::TY - ZH;
@@ -1439,6 +1443,71 @@ __device__ void cta_direct(const T* __restrict__ inv, int N, const T* b, T* z) {
         if (lane == 0) z[r] = s;
     }
     __syncthreads();
+}
+
+/** z = X b for a dense row-major N x N inverse X, one warp per row; b is
+ * staged in shared memory. The exact solve of a coarse level over the
+ * whole GPU. */
+template <typename T>
+__global__ void __launch_bounds__(256) direct_matvec_k(const T* __restrict__ X, int N, const T* __restrict__ b,
+                                                       T* __restrict__ z) {
+    extern __shared__ __align__(16) unsigned char dm_raw[];
+    T* sb = reinterpret_cast<T*>(dm_raw);
+    for (int k = threadIdx.x; k < N; k += blockDim.x) sb[k] = b[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (r >= N) return;
+    const T* row = X + size_t(r) * N;
+    T s0 = 0, s1 = 0;
+    int k = lane;
+    for (; k + 32 < N; k += 64) {
+        s0 += row[k] * sb[k];
+        s1 += row[k + 32] * sb[k + 32];
+    }
+    if (k < N) s0 += row[k] * sb[k];
+    T s = s0 + s1;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) z[r] = s;
+}
+
+__global__ void to_f32_k(const double* __restrict__ x, float* __restrict__ y, long n) {
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < n; k += long(gridDim.x) * blockDim.x)
+        y[k] = float(x[k]);
+}
+
+/** Gauss-Jordan inversion on the device, in place and without pivoting (the
+ * coarse FEM operators are symmetric positive definite once their Dirichlet
+ * rows, which hold only a diagonal, are eliminated first; those come first
+ * in the row order). A is assembled from nine stencil planes. */
+__global__ void gj_assemble_k(const double* __restrict__ S, int m, int n, double* __restrict__ A) {
+    const int N = m * n;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    const int j = k / m, i = k - j * m;
+    for (int d = 0; d < 9; d++) {
+        const int ii = i + d % 3 - 1, jj = j + d / 3 - 1;
+        if (ii < 0 || ii >= m || jj < 0 || jj >= n) continue;
+        A[size_t(k) * N + ii + size_t(m) * jj] += S[size_t(d) * N + k];
+    }
+}
+/** Step k: the scaled pivot row rk and the pivot column ck (old values). */
+__global__ void gj_pivot_k(const double* __restrict__ A, int N, int k, double* __restrict__ rk,
+                           double* __restrict__ ck, int* bad) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= N) return;
+    const double p = A[size_t(k) * N + k];
+    if (q == 0 && !(fabs(p) > 1e-300 && isfinite(p))) atomicOr(bad, 1);
+    rk[q] = (q == k ? 1. : A[size_t(k) * N + q]) / p;
+    ck[q] = q == k ? 0. : A[size_t(q) * N + k];
+}
+__global__ void gj_update_k(double* __restrict__ A, int N, int k, const double* __restrict__ rk,
+                            const double* __restrict__ ck) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (q >= N) return;
+    double* a = A + size_t(i) * N + q;
+    if (i == k) *a = rk[q];
+    else *a = (q == k ? 0. : *a) - ck[i] * rk[q];
 }
 
 /** Row loops of the CTA-resident levels: warp w takes rows w, w+nw, ...;
@@ -2027,6 +2096,13 @@ class MG {
     int dlev = -1;
     double* dinv64 = nullptr;
     float* dinv32 = nullptr;
+    // the level solved exactly over the whole GPU (GDIRECT_MAX; FEM by
+    // default, cell-centred systems with VDI_MG_MAC_DIRECT=1), or -1; both
+    // precisions' V-cycles then stop there
+    int gdlev = -1;
+    double* gdinv64 = nullptr;
+    float* gdinv32 = nullptr;
+    bool allow_gdirect = true;   // false where the inverse would need an allocation
     // the cluster-resident coarse cycle (mg_cluster.cuh) of the FP64 and FP32
     // V-cycles: its top level (-1: not used), CTAs and shared memory per CTA
     struct ClusterPlan {
@@ -2058,10 +2134,19 @@ class MG {
         dinv64 = nullptr;
         dinv32 = nullptr;
         dlev = -1;
+        free_gdirect();
         if (bproj) cudaFree(bproj);
         if (dmean) cudaFree(dmean);
         bproj = nullptr;
         dmean = nullptr;
+    }
+
+    void free_gdirect() {
+        if (gdinv64) cudaFree(gdinv64);
+        if (gdinv32) cudaFree(gdinv32);
+        gdinv64 = nullptr;
+        gdinv32 = nullptr;
+        gdlev = -1;
     }
 
     bool fem() const { return kind == VDI_MG_FEM; }
@@ -2245,6 +2330,11 @@ class MG {
         cl32 = plan_cluster<float>();
         if (cl64.top >= 0) nmulti64 = cl64.top;
         if (cl32.top >= 0) nmulti32 = cl32.top;
+        free_gdirect();
+        if (setup_gdirect() == VDI_OK && gdlev >= 0) {
+            nmulti32 = nmulti64 = gdlev;
+            cl64 = cl32 = ClusterPlan{};
+        }
         return VDI_OK;
     }
 
@@ -2399,6 +2489,83 @@ class MG {
     const double* dinv(double*) const { return dinv64; }
     const float* dinv(float*) const { return dinv32; }
 
+    /** The whole-GPU exact solve of a FEM hierarchy's first CTA-resident
+     * level, when it has more than DIRECT_MAX and at most GDIRECT_MAX
+     * unknowns (VDI_MG_FEM_DIRECT=0 turns it off): the level's operator is
+     * probed into a stencil and inverted on the device. A failed inversion
+     * leaves the single-CTA cycle in place. */
+    int setup_gdirect() {
+        if (!allow_gdirect || general || smooth_tail || neumann()) return VDI_OK;
+        int l = -1;
+        if (fem()) {
+            const char* e = getenv("VDI_MG_FEM_DIRECT");
+            if ((e && atoi(e) == 0) || nmulti64 < 1) return VDI_OK;
+            l = nmulti64;
+        } else {
+            // cell-centred: opt-in (VDI_MG_MAC_DIRECT=1), the first level
+            // small enough, in place of the cluster or single-CTA cycle
+            const char* e = getenv("VDI_MG_MAC_DIRECT");
+            if (!e || atoi(e) == 0) return VDI_OK;
+            for (int q = 1; q < nlev && l < 0; q++)
+                if (size(q) <= GDIRECT_MAX) l = q;
+            if (l < 0) return VDI_OK;
+        }
+        const long N = size(l);
+        if (N <= DIRECT_MAX || N > GDIRECT_MAX) return VDI_OK;
+        const int ml = lv[l].m, nl = lv[l].n;
+        double *S = nullptr, *A = nullptr, *rk = nullptr, *ck = nullptr;
+        int* bad = nullptr;
+        int st = VDI_OK;
+        auto fail = [&](int code) {
+            cudaGetLastError();
+            if (S) cudaFree(S);
+            if (A) cudaFree(A);
+            if (rk) cudaFree(rk);
+            if (ck) cudaFree(ck);
+            if (bad) cudaFree(bad);
+            return code;
+        };
+        if (cudaMalloc(&S, 9 * N * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&A, size_t(N) * N * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&rk, N * sizeof(double)) != cudaSuccess || cudaMalloc(&ck, N * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&bad, sizeof(int)) != cudaSuccess)
+            return fail(VDI_ERR_CUDA);
+        auto apply = [&](const double* z, double* y) -> int {
+            if (fem()) apply_k<double><<<nblk(N), 256>>>(femc<double>(l), z, y);
+            else apply_k<double><<<nblk(N), 256>>>(ccc<double>(l), z, y);
+            VDI_CUDA(cudaGetLastError());
+            return VDI_OK;
+        };
+        st = probe_stencil(ml, nl, S, apply);
+        if (st != VDI_OK) return fail(st);
+        if (cudaMemset(A, 0, size_t(N) * N * sizeof(double)) != cudaSuccess ||
+            cudaMemset(bad, 0, sizeof(int)) != cudaSuccess)
+            return fail(VDI_ERR_CUDA);
+        const int nb = int((N + 255) / 256);
+        gj_assemble_k<<<nb, 256>>>(S, ml, nl, A);
+        for (int k = 0; k < N; k++) {
+            gj_pivot_k<<<nb, 256>>>(A, int(N), k, rk, ck, bad);
+            gj_update_k<<<dim3(nb, unsigned(N)), 256>>>(A, int(N), k, rk, ck);
+        }
+        int hbad = 0;
+        if (cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return fail(VDI_ERR_CUDA);
+        if (hbad) return fail(VDI_OK);   // a zero pivot: keep the CTA cycle
+        float* X32 = nullptr;
+        if (cudaMalloc(&X32, size_t(N) * N * sizeof(float)) != cudaSuccess) return fail(VDI_ERR_CUDA);
+        to_f32_k<<<std::min(nblk(N * N), 4096), 256>>>(A, X32, N * N);
+        if (cudaDeviceSynchronize() != cudaSuccess) {
+            cudaFree(X32);
+            return fail(VDI_ERR_CUDA);
+        }
+        gdinv64 = A;
+        gdinv32 = X32;
+        A = nullptr;
+        gdlev = l;
+        return fail(VDI_OK);   // frees the scratch
+    }
+    const double* gdinv(double*) const { return gdinv64; }
+    const float* gdinv(float*) const { return gdinv32; }
+
     /** The direct coarsest solve: the first CTA-resident level with at most
      * DIRECT_MAX unknowns, its operator probed into a stencil and inverted. */
     int setup_direct() {
@@ -2449,6 +2616,13 @@ class MG {
             TileArgs<T> a = targs<T>(nullptr, z, b);
             a.zero_init = 1;
             launch_cc_tile<T, 0>(s, ccc<T>(l), a);
+            VDI_CUDA(cudaGetLastError());
+            return VDI_OK;
+        }
+        if (l == nmulti && gdlev == l) {
+            const int N = int(size(l));
+            direct_matvec_k<T><<<(N + 7) / 8, 256, size_t(N) * sizeof(T), s>>>(gdinv(static_cast<T*>(nullptr)), N,
+                                                                              b, z);
             VDI_CUDA(cudaGetLastError());
             return VDI_OK;
         }
@@ -2720,7 +2894,7 @@ int mg_coarse_cycle(const MG* mg, int precision, int* first, int* ctas) {
     }
     const auto& cp = f32 ? mg->cl32 : mg->cl64;
     *first = f32 ? mg->nmulti32 : mg->nmulti64;
-    *ctas = cp.top >= 0 ? cp.cs : 1;
+    *ctas = mg->gdlev >= 0 && mg->gdlev == *first ? 0 : (cp.top >= 0 ? cp.cs : 1);
     return VDI_OK;
 }
 int mg_tiled_levels(const MG* mg, int precision) {
@@ -3047,6 +3221,7 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
     MG* g = new MG();
     g->kind = k.kind; g->m = k.m; g->n = k.n; g->c1 = k.c1; g->c2 = k.c2; g->x_sym = k.x_sym;
     g->allow_cluster = false;   // its inverse would need an allocation
+    g->allow_gdirect = false;   // so would this one
     int st = g->build_levels();
     if (st == VDI_OK && g->general) {
         set_error("vdi_mg_solve_noalloc: a %dx%d grid needs the general hierarchy, which allocates", k.m, k.n);
