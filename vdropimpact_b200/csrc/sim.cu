@@ -35,10 +35,11 @@ struct vdi_sim {
     Grid g{};
     GasPrm gp{};
     double dt_reg = 0;
-    cudaStream_t s = nullptr, s_gas = nullptr, s_vy = nullptr;
+    cudaStream_t s = nullptr, s_gas = nullptr, s_vy = nullptr, s_guess = nullptr;
     bool own_stream = false;
     cudaEvent_t ev_fork = nullptr, ev_gas = nullptr, ev_vy = nullptr, ev_vy_done = nullptr;
     cudaEvent_t ev_adv = nullptr, ev_side = nullptr;   // advection done; side-stream work done
+    cudaEvent_t ev_guess = nullptr;                    // the MAC guess done
     std::vector<double*> bufs;
     Fields f{};
     Gas gas{};
@@ -54,6 +55,7 @@ struct vdi_sim {
     double* d_tm = nullptr;     // tracer positions x0, y0, x1, ... (2 * ntrace)
     double* d_vacc = nullptr;   // the non-inertial frame's velocity of a step
     double* d_time_aside = nullptr;   // clock for a gas-layer update run alone
+    double* d_time_start = nullptr;   // the clock at the start of a step (the MAC guess's)
     int* d_err = nullptr;
     GasStats* d_gstats = nullptr;
     MG* mg[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -108,9 +110,10 @@ int update_visc(vdi_sim* S, double dt) {
 
 /** mgs_common::initial_guess (mgs_common.cc:17-50) for one solver, or the
  * quadratic variant when the parameters ask for it, at time *d_time + tadd. */
-int guess(vdi_sim* S, cudaStream_t s, int which, double* z, double* zp, double* zp2, int n, double tadd = 0.) {
+int guess(vdi_sim* S, cudaStream_t s, int which, double* z, double* zp, double* zp2, int n, double tadd = 0.,
+          const double* clock = nullptr) {
     const int quad = S->prm.mg_guess == VDI_GUESS_QUADRATIC || S->prm.mg_guess == VDI_GUESS_LEARNED;
-    return launch_guess(s, z, zp, zp2, n, S->hist + which, S->d_time, tadd, quad, S->d_err);
+    return launch_guess(s, z, zp, zp2, n, S->hist + which, clock ? clock : S->d_time, tadd, quad, S->d_err);
 }
 
 /** Enqueues one fluid_2d::step_forward(dt) (fluid_2d.cc:93-405). */
@@ -122,15 +125,23 @@ int enqueue_step(vdi_sim* S, double dt) {
     // The gas layer runs on its own stream, overlapping the advection. The
     // same stream then takes the work that needs neither the advection's
     // output nor the MAC solve, off the main stream's path:
-    //  - the MAC guess (it needs the clock advanced by the gas layer);
     //  - once the advection has read the ghost cells, the far-field boundary
     //    kernel (it writes only ghost velocities, which nothing before the
     //    MAC correction reads, and the gas pressure);
     //  - the FEM guess, at the time the MAC correction will set (tadd = dt/2).
     // The main stream joins before the MAC correction, which advances the
     // clock, so the FEM guess has read it by then.
+    // The MAC guess runs on a third stream from the start of the step: it
+    // extrapolates to the time the gas layer sets (the step's starting
+    // clock, copied aside first because the gas layer advances it, plus
+    // dt/2: the same sum the gas layer forms), and the main stream joins it
+    // before the MAC solve.
+    VDI_CUDA(cudaMemcpyAsync(S->d_time_start, S->d_time, sizeof(double), cudaMemcpyDeviceToDevice, s));
     VDI_CUDA(cudaEventRecord(S->ev_fork, s));
     VDI_CUDA(cudaStreamWaitEvent(S->s_gas, S->ev_fork, 0));
+    VDI_CUDA(cudaStreamWaitEvent(S->s_guess, S->ev_fork, 0));
+    VDI_TRY(guess(S, S->s_guess, SOLVER_MAC, S->q, S->q_prev, S->q_prev2, mn, 0.5 * dt, S->d_time_start));
+    VDI_CUDA(cudaEventRecord(S->ev_guess, S->s_guess));
     // tracers first (fluid_2d.cc:98), before anything rewrites u, v or
     // their ghost cells
     VDI_TRY(launch_tracers(s, g, S->f, S->d_tm, S->prm.ntrace, dt));
@@ -139,7 +150,6 @@ int enqueue_step(vdi_sim* S, double dt) {
     // h is final for this step once the gas layer has updated it
     if (S->lcfg.mode != VDI_LIFTOFF_OFF)
         VDI_TRY(liftoff_launch(S->s_gas, S->gas.h, S->lcfg, S->d_lift, S->d_lhist, S->lcap, dt));
-    VDI_TRY(guess(S, S->s_gas, SOLVER_MAC, S->q, S->q_prev, S->q_prev2, mn));
     VDI_CUDA(cudaEventRecord(S->ev_gas, S->s_gas));
     if (S->fused_advect) {
         // stages 1-5 in one kernel, concurrent with the gas layer; the
@@ -160,6 +170,7 @@ int enqueue_step(vdi_sim* S, double dt) {
     VDI_TRY(launch_inviscid_bc(S->s_gas, g, S->f, S->gas, dt));
     VDI_TRY(guess(S, S->s_gas, SOLVER_FEM, S->zf, S->zf_prev, S->zf_prev2, nf, 0.5 * dt));
     VDI_CUDA(cudaEventRecord(S->ev_side, S->s_gas));
+    VDI_CUDA(cudaStreamWaitEvent(s, S->ev_guess, 0));
     if (S->prm.mg_guess == VDI_GUESS_LEARNED) {
         // the network corrects the extrapolated guess from its residual
         if (!S->unet) {
@@ -502,6 +513,8 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     }
     if (cudaStreamCreateWithFlags(&S->s_gas, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&S->s_vy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&S->s_guess, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_guess, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&S->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&S->ev_gas, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&S->ev_vy, cudaEventDisableTiming) != cudaSuccess ||
@@ -543,6 +556,7 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     if (P.ntrace > 0 && (st = alloc_zero(S, &S->d_tm, 2 * size_t(P.ntrace))) != VDI_OK) return fail(st);
     if ((st = alloc_zero(S, &S->d_vacc, 1)) != VDI_OK) return fail(st);
     if ((st = alloc_zero(S, &S->d_time_aside, 1)) != VDI_OK) return fail(st);
+    if ((st = alloc_zero(S, &S->d_time_start, 1)) != VDI_OK) return fail(st);
     double* ebuf;
     if ((st = alloc_zero(S, &ebuf, 1 + sizeof(GasStats) / 8 + 1)) != VDI_OK) return fail(st);
     S->d_err = reinterpret_cast<int*>(ebuf);
@@ -619,8 +633,10 @@ int vdi_sim_destroy(vdi_sim* S) {
     if (S->ev_vy_done) cudaEventDestroy(S->ev_vy_done);
     if (S->ev_adv) cudaEventDestroy(S->ev_adv);
     if (S->ev_side) cudaEventDestroy(S->ev_side);
+    if (S->ev_guess) cudaEventDestroy(S->ev_guess);
     if (S->s_gas) cudaStreamDestroy(S->s_gas);
     if (S->s_vy) cudaStreamDestroy(S->s_vy);
+    if (S->s_guess) cudaStreamDestroy(S->s_guess);
     if (S->own_stream && S->s) cudaStreamDestroy(S->s);
     delete S;
     return VDI_OK;
