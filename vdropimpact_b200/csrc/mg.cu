@@ -1700,28 +1700,24 @@ __device__ __forceinline__ void grid_ij(const OP& c, long k, int& i, int& j) {
     i = int(k - long(j) * op_m(c));
 }
 
-/** Grid-stride walk over the m-wide grid's points 0 <= k < tot: calls
- * f(k, i, j) with (i, j) advanced incrementally (two divisions per thread,
- * none per point). */
+/** Rows of one warp's strip in strip_walk. */
+static constexpr int STRIP_ROWS = 16;
+
+/** Walk over an m x n grid by strips of 32 columns and STRIP_ROWS rows, one
+ * warp per strip (warps take strips a grid's warps apart): lane t calls
+ * f(k, i, j) for column i = strip column + t down the strip's rows. The
+ * stencil's neighbours in rows j-1 and j+1 are the rows the same warp has
+ * just read or reads next, so they come from L1: z and b cross DRAM once. */
 template <class F>
-__device__ __forceinline__ void grid_walk(int m, long tot, F f) {
-    const long stride = long(gridDim.x) * blockDim.x;
-    long k = blockIdx.x * long(blockDim.x) + threadIdx.x;
-    if (k >= tot) return;
-    int j = int(k / m), i = int(k - long(j) * m);
-    const int sj = int(stride / m), si = int(stride - long(sj) * m);
-    // unrolled so that later points' loads issue before earlier points'
-    // arithmetic: a thread walks several points, and one load at a time
-    // leaves the memory system idle
+__device__ __forceinline__ void strip_walk(int m, int n, F f) {
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int sx = (m + 31) >> 5, sy = (n + STRIP_ROWS - 1) / STRIP_ROWS, ns = sx * sy;
+    for (int sidx = blockIdx.x * wpb + (threadIdx.x >> 5); sidx < ns; sidx += gridDim.x * wpb) {
+        const int sj = sidx / sx, i = (sidx - sj * sx) * 32 + lane;
+        if (i >= m) continue;
+        const int j0 = sj * STRIP_ROWS, j1 = min(j0 + STRIP_ROWS, n);
 #pragma unroll 4
-    for (; k < tot; k += stride) {
-        f(k, i, j);
-        i += si;
-        j += sj;
-        if (i >= m) {
-            i -= m;
-            j++;
-        }
+        for (int j = j0; j < j1; j++) f(long(j) * m + i, i, j);
     }
 }
 
@@ -1730,8 +1726,7 @@ template <typename T, class OP>
 __global__ void resid_norm_k(OP c, const T* __restrict__ z, const T* __restrict__ b, Reduce rd, SolveCtl* ctl,
                              int count_cycle, int use_cond, cudaGraphConditionalHandle h) {
     double s = 0;
-    const long tot = long(op_m(c)) * op_n(c);
-    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
+    strip_walk(op_m(c), op_n(c), [&](long k, int i, int j) {
         double r = double(op_resid(c, z + k, b[k], op_m(c), i, j));
         s += r * r;
     });
@@ -1750,7 +1745,7 @@ __global__ void first_check_k(OP c, T* __restrict__ z, const T* __restrict__ b, 
     __shared__ int zero_src;
     double sb = 0, sr = 0;
     const long tot = long(op_m(c)) * op_n(c);
-    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
+    strip_walk(op_m(c), op_n(c), [&](long k, int i, int j) {
         double bv = double(b[k]);
         double r = double(op_resid(c, z + k, b[k], op_m(c), i, j));
         sb += bv * bv;
@@ -1781,8 +1776,7 @@ __global__ void resid_to32_k(OP c, const double* __restrict__ z, const double* _
                              float* __restrict__ r32, Reduce rd, SolveCtl* ctl, int count_cycle, int use_cond,
                              cudaGraphConditionalHandle h) {
     double s = 0;
-    const long tot = long(op_m(c)) * op_n(c);
-    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
+    strip_walk(op_m(c), op_n(c), [&](long k, int i, int j) {
         double r = op_resid(c, z + k, b[k], op_m(c), i, j);
         r32[k] = float(r);
         s += r * r;
@@ -1806,8 +1800,7 @@ template <typename T, class OP>
 __global__ void resid_out_k(OP c, const T* __restrict__ z, const T* __restrict__ b, T* __restrict__ r, Reduce rd,
                             double* out) {
     double s = 0;
-    const long tot = long(op_m(c)) * op_n(c);
-    grid_walk(op_m(c), tot, [&](long k, int i, int j) {
+    strip_walk(op_m(c), op_n(c), [&](long k, int i, int j) {
         T v = op_resid(c, z + k, b[k], op_m(c), i, j);
         if (r) r[k] = v;
         s += double(v) * double(v);
@@ -1856,6 +1849,12 @@ static inline int resident_blocks() {
 /** Blocks of a whole-grid reduction over n points: one resident wave at
  * most, so the partial sums stay few and the last block's sum short. */
 static inline int rblocks(long n) { return std::max(1, std::min({MAX_PARTIALS, nblk(n, 256), resident_blocks()})); }
+/** Blocks of 256 threads for a strip_walk over an m x n grid: one warp per
+ * strip, one resident wave at most, few enough for grid_sum2's partials. */
+static inline int sblocks(int m, int n) {
+    const long strips = long((m + 31) / 32) * ((n + STRIP_ROWS - 1) / STRIP_ROWS);
+    return int(std::max(1L, std::min({long(MAX_PARTIALS / 2), (strips + 7) / 8, long(resident_blocks())})));
+}
 
 /** Per-level description in double precision, converted per precision. */
 struct LevelD {
@@ -2739,9 +2738,12 @@ class MG {
         return vcycle<float>(s, 0, b32[0], z32[0], nmulti32, z32, b32, smem32, 1, 0, 0, 0);
     }
 
+    /** sblocks for the finest level. */
+    int sblk0() const { return general ? sblocks(gen.gm[0], gen.gn[0]) : sblocks(lv[0].m, lv[0].n); }
+
     int enqueue_resid_norm(cudaStream_t s, const double* b, const double* z, int count_cycle, int use_cond,
                            cudaGraphConditionalHandle h) {
-        int nb = rblocks(size(0));
+        int nb = sblk0();
         if (general)
             resid_norm_k<double><<<nb, 256, 0, s>>>(gen.op(0), z, b, rd, ctl, count_cycle, use_cond, h);
         else if (fem())
@@ -2754,7 +2756,7 @@ class MG {
 
     int enqueue_resid32(cudaStream_t s, const double* b, const double* z, int count_cycle, int use_cond,
                         cudaGraphConditionalHandle h) {
-        int nb = rblocks(size(0));
+        int nb = sblk0();
         if (fem())
             resid_to32_k<<<nb, 256, 0, s>>>(femc<double>(0), z, b, b32[0], rd, ctl, count_cycle, use_cond, h);
         else
@@ -2804,7 +2806,7 @@ class MG {
             VDI_CUDA(cudaGetLastError());
             return enqueue_resid32(s, b, z, 0, use_cond, h);
         }
-        int nb = std::max(1, std::min({MAX_PARTIALS / 2, nblk(N, 256), resident_blocks()}));
+        int nb = sblk0();
         if (general)
             first_check_k<double><<<nb, 256, 0, s>>>(gen.op(0), z, b, rd, ctl, use_cond, h);
         else if (fem())
@@ -3001,7 +3003,7 @@ int mg_v_cycle(MG* mg, cudaStream_t s, const double* b, double* z) { return mg->
 int mg_residual(MG* mg, cudaStream_t s, const double* b, const double* z, double* r, double* norm) {
     double* d_out;
     VDI_CUDA(cudaMallocAsync(&d_out, sizeof(double), s));
-    int nb = rblocks(mg->size(0));
+    int nb = mg->sblk0();
     if (mg->fem())
         resid_out_k<double><<<nb, 256, 0, s>>>(mg->femc<double>(0), z, b, r, mg->rd, d_out);
     else
@@ -3107,7 +3109,7 @@ int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, do
 }
 
 int mg_residual_async(MG* mg, cudaStream_t s, const double* b, const double* z, double* r, double* d_norm) {
-    int nb = rblocks(mg->size(0));
+    int nb = mg->sblk0();
     if (mg->fem())
         resid_out_k<double><<<nb, 256, 0, s>>>(mg->femc<double>(0), z, b, r, mg->rd, d_norm);
     else

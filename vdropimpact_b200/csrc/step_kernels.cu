@@ -705,12 +705,14 @@ __global__ void k_frame_apply(double* __restrict__ v, long tot, const double* __
 // advances the clock by dt/2 passes tadd = dt/2 and gets the same double that
 // the clock will hold (the same single rounded addition).
 /** Points per thread of k_guess. */
-static constexpr int GUESS_PER = 4;
+static constexpr int GUESS_PER = 3;
 
 template <bool QUAD>
-__global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, double* __restrict__ zprev2, int n,
-                        GuessHist* h, const double* d_time, double tadd, int* err) {
+__global__ void __launch_bounds__(256, 4) k_guess(double* __restrict__ z, double* __restrict__ zprev,
+                                                  double* __restrict__ zprev2, int n, GuessHist* h,
+                                                  const double* d_time, double tadd, int* err) {
     __shared__ double s_t[4];   // t, t0, t_prev, t_prev2
+    __shared__ double s_w[3];   // the extrapolation's weights (their meaning by rule below)
     __shared__ int s_sc, s_head;
     // each thread takes GUESS_PER points, a grid-size apart; their values
     // are loaded before the history header is, so the two overlap
@@ -733,9 +735,31 @@ __global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, doub
         s_head = h->head;
     }
     __syncthreads();
+    {
+        // the extrapolation weights, once per block: thread q < 3 forms
+        // weight q (linear: z = w0 zz - w1 v1 with w0, w1 over one
+        // reciprocal; quadratic: the Lagrange weights, z = w0 zz + w1 v1 +
+        // w2 v2)
+        const double t = s_t[0], t0 = s_t[1], t1 = s_t[2], t2 = s_t[3];
+        const int q = threadIdx.x;
+        if (q < 3) s_w[q] = 0.;
+        if (q < 3 && s_sc >= 2 && !(fabs(t0 - t1) < 2.220446049250313e-16 * 10)) {
+            if (!QUAD || s_sc == 2) {
+                double a = 1. / (t0 - t1);
+                s_w[q] = q == 0 ? (t - t1) * a : (q == 1 ? (t - t0) * a : 0.);
+            } else {
+                const double tq = q == 0 ? t0 : (q == 1 ? t1 : t2);
+                const double ta = q == 0 ? t1 : t0, tb = q == 2 ? t1 : t2;
+                s_w[q] = (t - ta) * (t - tb) / ((tq - ta) * (tq - tb));
+            }
+        }
+    }
+    __syncthreads();
     const int sc = s_sc;
     const double t = s_t[0], t0 = s_t[1], t1 = s_t[2];
     const bool dup = fabs(t0 - t1) < 2.220446049250313e-16 * 10;
+    const bool lin = !QUAD || sc == 2;
+    const double w0 = s_w[0], w1 = s_w[1], w2 = s_w[2];
     // quadratic history: h1 holds the solution at t_prev, h2 the one at
     // t_prev2; the newest history replaces h2's and the two swap roles
     const bool swap = QUAD && s_head;
@@ -750,16 +774,8 @@ __global__ void k_guess(double* __restrict__ z, double* __restrict__ zprev, doub
             if (sc == 1) h1[k] = vz[u];
         } else if (!dup) {
             double zz = vz[u];
-            if (!QUAD || sc == 2) {
-                double a = 1. / (t0 - t1), b = (t - t1) * a, cc = (t - t0) * a;
-                z[k] = b * zz - cc * v1;
-            } else {
-                double t2 = s_t[3];
-                double l0 = (t - t1) * (t - t2) / ((t0 - t1) * (t0 - t2));
-                double l1 = (t - t0) * (t - t2) / ((t1 - t0) * (t1 - t2));
-                double l2 = (t - t0) * (t - t1) / ((t2 - t0) * (t2 - t1));
-                z[k] = l0 * zz + l1 * v1 + l2 * v2;
-            }
+            if (lin) z[k] = w0 * zz - w1 * v1;
+            else z[k] = w0 * zz + w1 * v1 + w2 * v2;
             if (QUAD) h2[k] = zz;
             else h1[k] = zz;
         }
