@@ -1445,35 +1445,57 @@ __device__ void cta_direct(const T* __restrict__ inv, int N, const T* b, T* z) {
     __syncthreads();
 }
 
-/** z = X b for a dense row-major N x N inverse X, one warp per row; b is
- * staged in shared memory. The exact solve of a coarse level over the
- * whole GPU. */
+/** z = X b for a dense row-major N x N inverse X with row pitch P (a
+ * multiple of 4, the pad zero), one warp per row: 16-byte loads, four
+ * independent partial sums per lane, so a warp keeps 2-4 KB of its row in
+ * flight. b is staged in shared memory (zero-padded to P). The exact solve
+ * of a coarse level over the whole GPU. */
 template <typename T>
-__global__ void __launch_bounds__(256) direct_matvec_k(const T* __restrict__ X, int N, const T* __restrict__ b,
-                                                       T* __restrict__ z) {
+__global__ void __launch_bounds__(256) direct_matvec_k(const T* __restrict__ X, int N, int P,
+                                                       const T* __restrict__ b, T* __restrict__ z) {
+    using V = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+    constexpr int E = int(sizeof(V) / sizeof(T));   // elements per vector
     extern __shared__ __align__(16) unsigned char dm_raw[];
     T* sb = reinterpret_cast<T*>(dm_raw);
-    for (int k = threadIdx.x; k < N; k += blockDim.x) sb[k] = b[k];
+    for (int k = threadIdx.x; k < P; k += blockDim.x) sb[k] = k < N ? b[k] : T(0);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (r >= N) return;
-    const T* row = X + size_t(r) * N;
-    T s0 = 0, s1 = 0;
-    int k = lane;
-    for (; k + 32 < N; k += 64) {
-        s0 += row[k] * sb[k];
-        s1 += row[k + 32] * sb[k + 32];
+    const V* row = reinterpret_cast<const V*>(X + size_t(r) * P);
+    const V* bv = reinterpret_cast<const V*>(sb);
+    const int nv = P / E;
+    T acc[4] = {0, 0, 0, 0};
+    int q = lane;
+    for (; q + 96 < nv; q += 128) {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const V x = __ldg(row + q + 32 * u), y = bv[q + 32 * u];
+            if constexpr (E == 2) acc[u] += x.x * y.x + x.y * y.y;
+            else acc[u] += x.x * y.x + x.y * y.y + x.z * y.z + x.w * y.w;
+        }
     }
-    if (k < N) s0 += row[k] * sb[k];
-    T s = s0 + s1;
+    for (; q < nv; q += 32) {
+        const V x = __ldg(row + q), y = bv[q];
+        if constexpr (E == 2) acc[0] += x.x * y.x + x.y * y.y;
+        else acc[0] += x.x * y.x + x.y * y.y + x.z * y.z + x.w * y.w;
+    }
+    T s = (acc[0] + acc[1]) + (acc[2] + acc[3]);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) z[r] = s;
 }
 
-__global__ void to_f32_k(const double* __restrict__ x, float* __restrict__ y, long n) {
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < n; k += long(gridDim.x) * blockDim.x)
-        y[k] = float(x[k]);
+/** Copies a dense N x N matrix into rows of pitch P >= N (zero pad), in
+ * FP64 and FP32. */
+__global__ void pad_rows_k(const double* __restrict__ A, int N, int P, double* __restrict__ X64,
+                           float* __restrict__ X32) {
+    const long tot = long(N) * P;
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < tot; k += long(gridDim.x) * blockDim.x) {
+        const long r = k / P, c = k - r * P;
+        const double v = c < N ? A[r * N + c] : 0.;
+        X64[k] = v;
+        X32[k] = float(v);
+    }
 }
 
 /** Gauss-Jordan inversion on the device, in place and without pivoting (the
@@ -2101,6 +2123,7 @@ class MG {
     int gdlev = -1;
     double* gdinv64 = nullptr;
     float* gdinv32 = nullptr;
+    int gdpitch = 0;             // their row pitch
     bool allow_gdirect = true;   // false where the inverse would need an allocation
     // the cluster-resident coarse cycle (mg_cluster.cuh) of the FP64 and FP32
     // V-cycles: its top level (-1: not used), CTAs and shared memory per CTA
@@ -2549,16 +2572,24 @@ class MG {
         int hbad = 0;
         if (cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return fail(VDI_ERR_CUDA);
         if (hbad) return fail(VDI_OK);   // a zero pivot: keep the CTA cycle
+        // rows padded to a multiple of 4 elements for 16-byte loads
+        const int P = int((N + 3) & ~3L);
+        double* X64 = nullptr;
         float* X32 = nullptr;
-        if (cudaMalloc(&X32, size_t(N) * N * sizeof(float)) != cudaSuccess) return fail(VDI_ERR_CUDA);
-        to_f32_k<<<std::min(nblk(N * N), 4096), 256>>>(A, X32, N * N);
+        if (cudaMalloc(&X64, size_t(N) * P * sizeof(double)) != cudaSuccess) return fail(VDI_ERR_CUDA);
+        if (cudaMalloc(&X32, size_t(N) * P * sizeof(float)) != cudaSuccess) {
+            cudaFree(X64);
+            return fail(VDI_ERR_CUDA);
+        }
+        pad_rows_k<<<std::min(nblk(long(N) * P), 4096), 256>>>(A, int(N), P, X64, X32);
         if (cudaDeviceSynchronize() != cudaSuccess) {
+            cudaFree(X64);
             cudaFree(X32);
             return fail(VDI_ERR_CUDA);
         }
-        gdinv64 = A;
+        gdinv64 = X64;
         gdinv32 = X32;
-        A = nullptr;
+        gdpitch = P;
         gdlev = l;
         return fail(VDI_OK);   // frees the scratch
     }
@@ -2620,8 +2651,8 @@ class MG {
         }
         if (l == nmulti && gdlev == l) {
             const int N = int(size(l));
-            direct_matvec_k<T><<<(N + 7) / 8, 256, size_t(N) * sizeof(T), s>>>(gdinv(static_cast<T*>(nullptr)), N,
-                                                                              b, z);
+            direct_matvec_k<T><<<(N + 7) / 8, 256, size_t(gdpitch) * sizeof(T), s>>>(
+                gdinv(static_cast<T*>(nullptr)), N, gdpitch, b, z);
             VDI_CUDA(cudaGetLastError());
             return VDI_OK;
         }
