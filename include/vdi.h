@@ -355,8 +355,10 @@ int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* 
  * hierarchy has none) and the CTAs of that launch (1: a single CTA; 8 or
  * 16: a thread-block cluster whose CTAs hold row slabs of every level; 0:
  * that level is solved exactly by a dense inverse applied over the whole
- * GPU, as FEM hierarchies do when it has at most 3072 unknowns). No
- * reference counterpart. */
+ * GPU, as FEM hierarchies do when it has at most 3072 unknowns; -1: that
+ * level is solved exactly by cosine transforms in x and one tridiagonal
+ * system per mode in y, as separable MAC and FEM hierarchies do at their
+ * first level of at most 40000 unknowns). No reference counterpart. */
 int vdi_mg_coarse_cycle(const vdi_mg* mg, int precision, int* first_level, int* ctas);
 /* Which kernel runs the tiled levels, read once per process from
  * VDI_MG_TILE: 0 the shared-memory tiles (default), 1 register-blocked

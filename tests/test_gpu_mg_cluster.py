@@ -28,10 +28,13 @@ CASES = [(2048, 1024, 3, 16), (512, 256, 1, 16), (256, 128, 0, 16), (64, 32, 0, 
 
 
 def _system(V, m, n, cluster, monkeypatch):
+    # the separable transform solve would take the coarse levels instead
+    monkeypatch.setenv("VDI_MG_FAST_COARSE", "0")
     monkeypatch.setenv("VDI_MG_CLUSTER", "1" if cluster else "0")
     dx = 1.0 / m
     s = V.MgsMac(m, n, dx, 1.5 * dx)
     monkeypatch.delenv("VDI_MG_CLUSTER")
+    monkeypatch.delenv("VDI_MG_FAST_COARSE")
     return s
 
 
@@ -82,11 +85,13 @@ def test_cluster_cycle_reports_single_cta_for_other_systems(V, monkeypatch):
     the FEM one solves its first CTA-sized level (65x33 here) exactly over
     the whole GPU (0 CTAs), or runs the single-CTA cycle with
     VDI_MG_FEM_DIRECT=0."""
+    monkeypatch.setenv("VDI_MG_FAST_COARSE", "0")
     fem = V.MgsFem(129, 65, 1 / 128, 1 / 128)
     assert fem.coarse_cycle() == (1, 0)
     monkeypatch.setenv("VDI_MG_FEM_DIRECT", "0")
     fem = V.MgsFem(129, 65, 1 / 128, 1 / 128)
     monkeypatch.delenv("VDI_MG_FEM_DIRECT")
+    monkeypatch.delenv("VDI_MG_FAST_COARSE")
     assert fem.coarse_cycle() == (1, 1)
     neu = V.MgsMacNeumann(256, 128, 1 / 256, 1 / 256)
     assert neu.coarse_cycle()[1] == 1
@@ -112,9 +117,11 @@ def test_fem_direct_coarse_solve_matches_cta_cycle(V, M, N, first, prec, monkeyp
     b[:M] = 0.3
     res = {}
     for direct in (True, False):
+        monkeypatch.setenv("VDI_MG_FAST_COARSE", "0")
         monkeypatch.setenv("VDI_MG_FEM_DIRECT", "1" if direct else "0")
         s = V.MgsFem(M, N, 1.0 / (M - 1), 1.5 / (M - 1))
         monkeypatch.delenv("VDI_MG_FEM_DIRECT")
+        monkeypatch.delenv("VDI_MG_FAST_COARSE")
         f, ctas = s.coarse_cycle(precision=prec if prec == "mixed" else None)
         if direct:
             assert (f, ctas) == (first, 0)

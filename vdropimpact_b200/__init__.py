@@ -481,9 +481,10 @@ class _MgSystem:
         return ms.value, by.value
 
     def coarse_cycle(self, precision=None):
-        """(first level, CTAs) of the single-launch coarse cycle of a V-cycle
-        in this precision: CTAs 1 for one CTA, 8 or 16 for a cluster; first
-        level -1 when the hierarchy has none."""
+        """(first level, CTAs) of the coarse path of a V-cycle in this
+        precision: CTAs 1 for one CTA, 8 or 16 for a cluster, 0 for the
+        dense-inverse solve over the whole GPU, -1 for the separable
+        transform solve; first level -1 when the hierarchy has none."""
         first, ctas = C.c_int(), C.c_int()
         check(lib().vdi_mg_coarse_cycle(self._h, _PREC[precision or self.precision], C.byref(first),
                                         C.byref(ctas)), "vdi_mg_coarse_cycle")

@@ -48,7 +48,11 @@ static constexpr int DIRECT_MAX = 256;
 // A FEM hierarchy whose first CTA-resident level has more than DIRECT_MAX but
 // at most GDIRECT_MAX unknowns solves that level exactly with a dense
 // inverse applied by the whole GPU, in place of the single-CTA cycle.
-static constexpr int GDIRECT_MAX = 3072;   // a 75 MB FP64 inverse at most
+static constexpr int GDIRECT_MAX = 3072;
+// A hierarchy whose operator is separable solves its first level of at most
+// FAST_MAX unknowns exactly by cosine transforms in x and tridiagonal solves
+// in y (mg_fast.cuh), in place of every coarser level.
+static constexpr long FAST_MAX = 40000;   // a 75 MB FP64 inverse at most
 
 // ------------------------------------------------------------------ reduce
 __device__ __forceinline__ double warp_sum(double v) {
@@ -2086,6 +2090,7 @@ __global__ void sub_mean_k(const double* src, double* dst, long N, const double*
 
 #include "mg_general.cuh"
 #include "mg_cluster.cuh"
+#include "mg_fast.cuh"
 
 class MG {
   public:
@@ -2125,6 +2130,11 @@ class MG {
     float* gdinv32 = nullptr;
     int gdpitch = 0;             // their row pitch
     bool allow_gdirect = true;   // false where the inverse would need an allocation
+    // the level solved exactly by the separable transform solve, or -1
+    int fclev = -1, fc_j0 = 0, fc_rp = 0, fc_steps = 0;
+    FastArrays<double> fc64;
+    FastArrays<float> fc32;
+    bool allow_fast = true;      // false where its arrays would need an allocation
     // the cluster-resident coarse cycle (mg_cluster.cuh) of the FP64 and FP32
     // V-cycles: its top level (-1: not used), CTAs and shared memory per CTA
     struct ClusterPlan {
@@ -2157,11 +2167,20 @@ class MG {
         dinv32 = nullptr;
         dlev = -1;
         free_gdirect();
+        free_fast();
         if (bproj) cudaFree(bproj);
         if (dmean) cudaFree(dmean);
         bproj = nullptr;
         dmean = nullptr;
     }
+
+    void free_fast() {
+        fc64.release();
+        fc32.release();
+        fclev = -1;
+    }
+    const FastArrays<double>& fcarr(double*) const { return fc64; }
+    const FastArrays<float>& fcarr(float*) const { return fc32; }
 
     void free_gdirect() {
         if (gdinv64) cudaFree(gdinv64);
@@ -2353,7 +2372,11 @@ class MG {
         if (cl64.top >= 0) nmulti64 = cl64.top;
         if (cl32.top >= 0) nmulti32 = cl32.top;
         free_gdirect();
-        if (setup_gdirect() == VDI_OK && gdlev >= 0) {
+        free_fast();
+        if (setup_fast() == VDI_OK && fclev >= 0) {
+            nmulti32 = nmulti64 = fclev;
+            cl64 = cl32 = ClusterPlan{};
+        } else if (setup_gdirect() == VDI_OK && gdlev >= 0) {
             nmulti32 = nmulti64 = gdlev;
             cl64 = cl32 = ClusterPlan{};
         }
@@ -2511,6 +2534,76 @@ class MG {
     const double* dinv(double*) const { return dinv64; }
     const float* dinv(float*) const { return dinv32; }
 
+    /** The separable exact solve (mg_fast.cuh) of the first level with at
+     * most FAST_MAX unknowns, when the operator there is separable in the
+     * cosine basis of its centring (VDI_MG_FAST_COARSE=0 turns it off). A
+     * solve of a random source is checked against the operator before it is
+     * used; any failure leaves the other coarse paths. */
+    int setup_fast() {
+        const char* e = getenv("VDI_MG_FAST_COARSE");
+        if ((e && atoi(e) == 0) || !allow_fast || general || smooth_tail || neumann()) return VDI_OK;
+        // VDI_MG_FAST_MAX overrides the size bound (measurements)
+        const char* em = getenv("VDI_MG_FAST_MAX");
+        const long fmax = em && atol(em) > 0 ? atol(em) : FAST_MAX;
+        int l = -1;
+        for (int q = 1; q < nlev && l < 0; q++)
+            if (size(q) <= fmax) l = q;
+        if (l < 0) return VDI_OK;
+        const int ml = lv[l].m, nl = lv[l].n;
+        const long N = size(l);
+        if (ml > 2048) return VDI_OK;   // bounds the two m x m basis matrices
+        double *S = nullptr, *zt = nullptr, *bt = nullptr, *yt = nullptr;
+        auto done = [&](int code) {
+            cudaGetLastError();
+            for (double* p : {S, zt, bt, yt})
+                if (p) cudaFree(p);
+            if (fclev < 0) {
+                fc64.release();
+                fc32.release();
+            }
+            return code;
+        };
+        if (cudaMalloc(&S, 9 * N * sizeof(double)) != cudaSuccess) return done(VDI_ERR_CUDA);
+        auto apply = [&](const double* z, double* y) -> int {
+            if (fem()) apply_k<double><<<nblk(N), 256>>>(femc<double>(l), z, y);
+            else apply_k<double><<<nblk(N), 256>>>(ccc<double>(l), z, y);
+            VDI_CUDA(cudaGetLastError());
+            return VDI_OK;
+        };
+        if (probe_stencil(ml, nl, S, apply) != VDI_OK) return done(VDI_OK);
+        std::vector<double> Sh(9 * size_t(N));
+        if (cudaMemcpy(Sh.data(), S, Sh.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return done(VDI_ERR_CUDA);
+        FastHost F;
+        if (!fast_analyse(Sh, ml, nl, fem(), F)) return done(VDI_OK);
+        if (fast_upload<double>(F, fc64) != VDI_OK || fast_upload<float>(F, fc32) != VDI_OK) return done(VDI_ERR_CUDA);
+        // check: A (A^-1 b) = b for a pseudo-random source
+        std::vector<double> bh(N), yh(N);
+        unsigned r = 12345u;
+        for (long k = 0; k < N; k++) {
+            r = r * 1664525u + 1013904223u;
+            bh[k] = double(r >> 8) / double(1u << 24) - 0.5;
+        }
+        if (cudaMalloc(&zt, N * sizeof(double)) != cudaSuccess || cudaMalloc(&bt, N * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&yt, N * sizeof(double)) != cudaSuccess ||
+            cudaMemcpy(bt, bh.data(), N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+            return done(VDI_ERR_CUDA);
+        if (fast_solve<double>(0, fc64, ml, nl, F.j0, F.rp, F.steps, bt, zt) != VDI_OK || apply(zt, yt) != VDI_OK ||
+            cudaMemcpy(yh.data(), yt, N * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return done(VDI_ERR_CUDA);
+        double err = 0, bmax = 0;
+        for (long k = 0; k < N; k++) {
+            err = std::max(err, std::fabs(yh[k] - bh[k]));
+            bmax = std::max(bmax, std::fabs(bh[k]));
+        }
+        if (!(err <= 1e-10 * bmax)) return done(VDI_OK);
+        fclev = l;
+        fc_j0 = F.j0;
+        fc_rp = F.rp;
+        fc_steps = F.steps;
+        return done(VDI_OK);
+    }
+
     /** The whole-GPU exact solve of a FEM hierarchy's first CTA-resident
      * level, when it has more than DIRECT_MAX and at most GDIRECT_MAX
      * unknowns (VDI_MG_FEM_DIRECT=0 turns it off): the level's operator is
@@ -2649,6 +2742,8 @@ class MG {
             VDI_CUDA(cudaGetLastError());
             return VDI_OK;
         }
+        if (l == nmulti && fclev == l)
+            return fast_solve<T>(s, fcarr(static_cast<T*>(nullptr)), lv[l].m, lv[l].n, fc_j0, fc_rp, fc_steps, b, z);
         if (l == nmulti && gdlev == l) {
             const int N = int(size(l));
             direct_matvec_k<T><<<(N + 7) / 8, 256, size_t(gdpitch) * sizeof(T), s>>>(
@@ -2927,7 +3022,8 @@ int mg_coarse_cycle(const MG* mg, int precision, int* first, int* ctas) {
     }
     const auto& cp = f32 ? mg->cl32 : mg->cl64;
     *first = f32 ? mg->nmulti32 : mg->nmulti64;
-    *ctas = mg->gdlev >= 0 && mg->gdlev == *first ? 0 : (cp.top >= 0 ? cp.cs : 1);
+    *ctas = mg->fclev >= 0 && mg->fclev == *first ? -1
+            : (mg->gdlev >= 0 && mg->gdlev == *first ? 0 : (cp.top >= 0 ? cp.cs : 1));
     return VDI_OK;
 }
 int mg_tiled_levels(const MG* mg, int precision) {
@@ -3255,6 +3351,7 @@ int noalloc_build(const NoallocKey& k, unsigned char* base, MG** out) {
     g->kind = k.kind; g->m = k.m; g->n = k.n; g->c1 = k.c1; g->c2 = k.c2; g->x_sym = k.x_sym;
     g->allow_cluster = false;   // its inverse would need an allocation
     g->allow_gdirect = false;   // so would this one
+    g->allow_fast = false;      // and the transform solve's arrays
     int st = g->build_levels();
     if (st == VDI_OK && g->general) {
         set_error("vdi_mg_solve_noalloc: a %dx%d grid needs the general hierarchy, which allocates", k.m, k.n);
