@@ -8,11 +8,14 @@ solves, FEM multigrid projection. Solver configurations timed on the same
 workload:
   plain     - FP64 V-cycles, linear time-extrapolated initial guess (the
               reference's method on the GPU)
-  fast      - the headline: by default FP64 V-cycles with the quadratic
-              time-extrapolated guess, the fastest measured configuration
-  variants  - FP32 coarse-grid corrections (hybrid), FP32 V-cycles in FP64
-              iterative refinement (mixed), and the learned U-Net guess with
-              the refined V-cycles (learned_mixed), over fewer steps
+  fast      - the headline: by default FP32 V-cycles in FP64 iterative
+              refinement with the quadratic time-extrapolated guess, the
+              fastest measured configuration (every solve still stops on the
+              FP64 residual)
+  variants  - the other configurations on the same steps: FP32 coarse-grid
+              corrections (hybrid), FP64 V-cycles (fp64), FP32 V-cycles in
+              FP64 refinement (mixed, when not the headline), and the learned
+              U-Net guess with the refined V-cycles (learned_mixed)
 `value` is the headline configuration's steps/s, summed over ranks (each
 rank runs an independent replica of the simulation).
 
@@ -50,7 +53,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only", default="", help="run only 'plain' or 'fast' (profiling)")
     ap.add_argument("--eager", action="store_true", help="launch kernels without CUDA graphs (profiling)")
-    ap.add_argument("--fast-precision", default="fp64", choices=["fp64", "mixed", "hybrid"])
+    ap.add_argument("--fast-precision", default="mixed", choices=["fp64", "mixed", "hybrid"],
+                    help="the headline configuration's V-cycles (mixed: FP32 V-cycles in FP64 refinement, "
+                         "the fastest measured)")
     ap.add_argument("--fast-guess", default="quadratic", choices=["linear", "quadratic", "learned"])
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes instead of the autotuned ones")
@@ -259,24 +264,40 @@ def measured_peak_gbs():
 # capture of the same kernel on a 4096x2048 grid (192.3 MB per launch),
 # scaled to the 2048x1024 bench grid by the number of cells.
 CC_POST_DRAM_BYTES = 192.3e6 / 4
+# The same for the FP32 post-smoothing tile of the refinement's V-cycles,
+# captured inside the bench's own 2048x1024 step (reads 18.9 MB: z, b and the
+# coarse correction; its 8 MB of writes stay in the L2 within the launch).
+CC_POST32_DRAM_BYTES = 18.92e6
 
 
 def roofline(V, torch, args):
-    """The dominant kernel of the step: the finest-level post-smoothing tile
-    kernel of the cell-centred solves (MAC and both viscous systems), timed
-    with CUDA events on its own stream over repeated launches at the bench
-    grid. Algorithmic bytes per launch: z in, b in, z out (8 B each per cell)
-    plus the coarse correction (8 B per coarse cell)."""
+    """The dominant kernel of the step, timed with CUDA events on its own
+    stream over repeated launches at the bench grid: the finest-level
+    post-smoothing tile kernel of the cell-centred solves (MAC and both
+    viscous systems), in the headline's V-cycle precision. Algorithmic
+    bytes per launch: z in, b in, z out plus the coarse correction, 8 bytes
+    a value in FP64 V-cycles, 4 in the FP32 V-cycles of the refinement."""
     m, n = (int(x) for x in args.grid.split("x"))
     s = V.MgsMac(m, n, 1.0 / m, 1.0 / m)
     g = torch.Generator(device="cuda").manual_seed(0)
     s.b.copy_(torch.randn(m * n, dtype=torch.float64, device="cuda", generator=g))
-    ms, nbytes = s.profile(1, 100)
+    f32 = args.fast_precision == "mixed"
+    ms, nbytes = s.profile(5 if f32 else 1, 100)
     peak, kind = measured_peak_gbs()
     achieved = nbytes / (ms * 1e-3) / 1e9
-    return {"kernel": "cc_tile<double, POST> on the 2048x1024 MAC grid", "bound": "hbm", "achieved": achieved,
-            "peak": peak, "peak_source": kind, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": CC_POST_DRAM_BYTES, "algorithmic_bytes": nbytes, "ms_per_launch": ms}
+    name = "cc_tile<float, POST> (FP32 V-cycle of the refinement)" if f32 else "cc_tile<double, POST>"
+    out = {"kernel": f"{name} on the {args.grid} MAC grid", "bound": "hbm", "achieved": achieved,
+           "peak": peak, "peak_source": kind, "unit": "GB/s", "frac": achieved / peak,
+           "traffic": CC_POST32_DRAM_BYTES if f32 else CC_POST_DRAM_BYTES, "algorithmic_bytes": nbytes,
+           "ms_per_launch": ms}
+    if f32:
+        # the FP64 tile of the FP64 configurations, for comparison
+        ms64, nb64 = s.profile(1, 100)
+        a64 = nb64 / (ms64 * 1e-3) / 1e9
+        out["fp64_tile"] = {"kernel": f"cc_tile<double, POST> on the {args.grid} MAC grid", "achieved": a64,
+                            "frac": a64 / peak, "traffic": CC_POST_DRAM_BYTES, "algorithmic_bytes": nb64,
+                            "ms_per_launch": ms64}
+    return out
 
 
 # Canonical algorithmic bytes of the step's work outside the multigrid
@@ -471,13 +492,15 @@ def main():
         line["speedup_vs_plain_fp64"] = p["ms"] / head["ms"]
     if not args.no_variants and not args.only and ws == 1:
         # the other solver configurations of the metric, on the same workload:
-        # FP32 coarse-grid corrections, FP32 V-cycles in FP64 refinement, and
-        # the learned guess with the refined V-cycles
+        # FP32 coarse-grid corrections, FP32 V-cycles in FP64 refinement, FP64
+        # V-cycles, and the learned guess with the refined V-cycles
         vsteps = args.steps
         variants = {}
-        for name, prec, guess in (("hybrid_quadratic", "hybrid", "quadratic"),
-                                  ("mixed_quadratic", "mixed", "quadratic"),
-                                  ("learned_mixed", "mixed", "learned")):
+        others = [("hybrid_quadratic", "hybrid", "quadratic"), ("mixed_quadratic", "mixed", "quadratic"),
+                  ("fp64_quadratic", "fp64", "quadratic"), ("learned_mixed", "mixed", "learned")]
+        # the headline's own configuration is not timed twice
+        others = [o for o in others if (o[1], o[2]) != (args.fast_precision, args.fast_guess)]
+        for name, prec, guess in others:
             net = train_guess_net(V, torch, text, args) if guess == "learned" else None
             fv, _, msv, vcv, _, _, _ = time_config(V, torch, text, args, prec, guess, stream, ws, net=net,
                                                   steps=vsteps)

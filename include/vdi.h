@@ -346,8 +346,11 @@ int vdi_mg_apply(vdi_mg* mg, const double* d_z, double* d_y);
  * events on the system's stream, which = 0 the finest-level
  * pre-smoothing/restriction kernel, 1 the finest prolongation/post-smoothing
  * kernel, 2 a whole FP64 V-cycle (the ms per V-cycle that mg_test.cc:36-43
- * reports), 3 the single-launch coarse cycle alone; returns the mean
- * duration and the algorithmic bytes per launch (0 for which = 3). */
+ * reports), 3 the single-launch coarse cycle alone; in the mixed precision's
+ * refinement, 4 the finest FP32 pre-smoothing kernel (from zero), 5 the
+ * finest FP32 post-smoothing kernel, 6 the FP64 residual pass that writes
+ * the FP32 source; returns the mean duration and the algorithmic bytes per
+ * launch (0 for which = 3). */
 int vdi_mg_profile(vdi_mg* mg, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
                    double* bytes_per_launch);
 /* The coarse levels of a V-cycle (of the given vdi_mg_precision) that run in

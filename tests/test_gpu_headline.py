@@ -4,10 +4,10 @@ CPU multigrid that stops at ||b-Az||/||b|| <= 1e-10).
 
 - The liquid-deposition case (sims/ld_vis100.cfg physics) on its 2048x1024
   grid with a 2048-cell gas layer: 100 steps of fluid_2d::step_forward
-  (fluid_2d.cc:93-405) from init_fields, with the solver configuration that
-  is timed (FP64 V-cycles, quadratic time-extrapolated guess, autotuned
-  launch shapes and hierarchy cuts, CUDA-graph steps, the MAC's cluster
-  coarse cycle).
+  (fluid_2d.cc:93-405) from init_fields, with the solver configurations
+  that are timed (FP64 V-cycles, and FP32 V-cycles in FP64 refinement; the
+  quadratic time-extrapolated guess, autotuned launch shapes and hierarchy
+  cuts, CUDA-graph steps, the separable exact coarse solve).
 - Members of a batched viscosity sweep at 512x256 and 1024x512 (the sweep of
   sims/create_cfg.pl:11), stepped together in one batch with FP32 V-cycles
   in FP64 refinement, each against its own reference run.
@@ -82,10 +82,21 @@ def field_errors(a, b):
     return out
 
 
-def test_liquid_deposition_2048x1024_matches_reference(V, ref_driver, tmp_path):
+LD_STEPS = 100
+
+
+@pytest.fixture(scope="module")
+def ld_reference(ref_driver, tmp_path_factory):
+    """The reference's 100 steps of the 2048x1024 case, run once."""
     text = cfg_text("ld_vis100.cfg", 2048, 1024)
-    nsteps = 100
-    f = V.Fluid2D(text, mg_rtol=1e-10, mg_guess="quadratic", graph=True)
+    return reference_state(ref_driver, tmp_path_factory.mktemp("ld"), "ld", text, LD_STEPS)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_liquid_deposition_2048x1024_matches_reference(V, ld_reference, precision):
+    text = cfg_text("ld_vis100.cfg", 2048, 1024)
+    nsteps = LD_STEPS
+    f = V.Fluid2D(text, mg_rtol=1e-10, mg_precision=precision, mg_guess="quadratic", graph=True)
     f.autotune()
     f.init_fields()
     dt = f.frame_dt()
@@ -93,10 +104,10 @@ def test_liquid_deposition_2048x1024_matches_reference(V, ref_driver, tmp_path):
     a = f.state()
     st = f.stats()
     f.close()
-    r = reference_state(ref_driver, tmp_path, "ld", text, nsteps)
+    r = ld_reference
     assert a["time"] == pytest.approx(r["time"], rel=1e-14)
     e = field_errors(a, r)
-    print("2048x1024 ld_vis100, 100 steps:", e, "V-cycles", st["vcycles"])
+    print(f"2048x1024 ld_vis100, 100 steps, {precision}:", e, "V-cycles", st["vcycles"])
     assert e.pop("tau_over_h") < TOL_TAU_OVER_H
     assert max(e.values()) < TOL, e
     assert st["solves"]["MAC"] == nsteps and st["solves"]["FEM"] == nsteps

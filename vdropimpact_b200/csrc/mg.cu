@@ -3171,7 +3171,53 @@ double mg_vcycle_bytes(const MG* mg, int fine_word, int coarse_word) {
 }
 
 int mg_profile(MG* mg, cudaStream_t s, int which, int iters, const double* b, double* z, float* ms, double* bytes) {
-    if (iters < 1 || which < 0 || which > 3) return VDI_ERR_INVALID_ARGUMENT;
+    if (iters < 1 || which < 0 || which > 6) return VDI_ERR_INVALID_ARGUMENT;
+    if (which >= 4) {
+        // the refinement's (mixed precision) finest kernels: 4 the FP32
+        // PRE from zero, 5 the FP32 POST, 6 the FP64 residual pass that
+        // writes the FP32 source and decides
+        if (mg->general || mg->nmulti32 < 1) return VDI_ERR_INVALID_ARGUMENT;
+        TileArgs<float> a = mg->targs<float>(which == 4 ? nullptr : mg->t32[0], which == 4 ? mg->t32[0] : mg->z32[0],
+                                             mg->b32[0]);
+        a.zero_init = which == 4;
+        a.bc = mg->b32[1];
+        a.zc = mg->z32[1];
+        auto launch = [&]() -> int {
+            if (which == 6) return mg->enqueue_resid32(s, b, z, 0, 0, 0);
+            if (mg->fem()) {
+                if (which == 4) launch_fem_tile<float, 0>(s, mg->femc<float>(0), a);
+                else launch_fem_tile<float, 1>(s, mg->femc<float>(0), a);
+            } else {
+                if (which == 4) launch_cc_tile<float, 0>(s, mg->ccc<float>(0), a);
+                else launch_cc_tile<float, 1>(s, mg->ccc<float>(0), a);
+            }
+            VDI_CUDA(cudaGetLastError());
+            return VDI_OK;
+        };
+        // one refinement iteration fills the FP32 source and coarse arrays
+        VDI_TRY(mg->enqueue_resid32(s, b, z, 0, 0, 0));
+        VDI_TRY(mg->vcycle32(s));
+        VDI_TRY(launch());
+        cudaEvent_t e0, e1;
+        VDI_CUDA(cudaEventCreate(&e0));
+        VDI_CUDA(cudaEventCreate(&e1));
+        VDI_CUDA(cudaEventRecord(e0, s));
+        int st = VDI_OK;
+        for (int k = 0; k < iters && st == VDI_OK; k++) st = launch();
+        VDI_CUDA(cudaEventRecord(e1, s));
+        VDI_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        VDI_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        VDI_TRY(st);
+        *ms = t / iters;
+        const double N = double(mg->size(0)), Nc = double(mg->size(1));
+        // 4: b in, z out, coarse source out; 5: z, b in, z out, coarse
+        // correction in (4 bytes each); 6: z, b in (8 bytes), source out (4)
+        *bytes = which == 4 ? 8 * N + 4 * Nc : (which == 5 ? 12 * N + 4 * Nc : 20 * N);
+        return VDI_OK;
+    }
     if (which >= 2) {
         // 2: whole FP64 V-cycles back to back (mg_test.cc:36-43 times the
         // same); 3: the single-CTA coarse cycle alone

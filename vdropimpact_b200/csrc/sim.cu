@@ -1185,7 +1185,7 @@ int vdi_mg_tile_path(long long* persistent_launches) { return mg_tile_path(persi
 
 int vdi_mg_profile(vdi_mg* h, int which, int iters, const double* d_b, double* d_z, float* ms_per_launch,
                    double* bytes_per_launch) {
-    if (!h || !d_b || !d_z || !ms_per_launch || !bytes_per_launch || which < 0 || which > 3)
+    if (!h || !d_b || !d_z || !ms_per_launch || !bytes_per_launch || which < 0 || which > 6)
         return VDI_ERR_INVALID_ARGUMENT;
     return mg_profile(h->g, h->s, which, iters, d_b, d_z, ms_per_launch, bytes_per_launch);
 }
