@@ -1764,16 +1764,19 @@ __global__ void resid_norm_k(OP c, const T* __restrict__ z, const T* __restrict_
 /** The start of a solve in one pass: ||b||^2 and ||b - A z0||^2, then the
  * first decision. A zero source is done at once with z = 0 (the shim and
  * this library agree on that convention): the last block, which every other
- * block has finished reading z before, zeroes it. */
+ * block has finished reading z before, zeroes it. With r32 (mixed
+ * precision) the residual is also written in FP32, the source of the first
+ * FP32 V-cycle. */
 template <typename T, class OP>
 __global__ void first_check_k(OP c, T* __restrict__ z, const T* __restrict__ b, Reduce rd, SolveCtl* ctl,
-                              int use_cond, cudaGraphConditionalHandle h) {
+                              int use_cond, cudaGraphConditionalHandle h, float* __restrict__ r32 = nullptr) {
     __shared__ int zero_src;
     double sb = 0, sr = 0;
     const long tot = long(op_m(c)) * op_n(c);
     strip_walk(op_m(c), op_n(c), [&](long k, int i, int j) {
         double bv = double(b[k]);
         double r = double(op_resid(c, z + k, b[k], op_m(c), i, j));
+        if (r32) r32[k] = float(r);
         sb += bv * bv;
         sr += r * r;
     });
@@ -1834,27 +1837,6 @@ __global__ void resid_out_k(OP c, const T* __restrict__ z, const T* __restrict__
     s = block_sum(s);
     double total;
     if (grid_sum(s, rd, &total) && threadIdx.x == 0) *out = sqrt(total);
-}
-
-__global__ void norm2_kernel(const double* __restrict__ x, long n, Reduce rd, SolveCtl* ctl) {
-    double s = 0;
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < n; k += long(gridDim.x) * blockDim.x)
-        s += x[k] * x[k];
-    s = block_sum(s);
-    double total;
-    if (grid_sum(s, rd, &total) && threadIdx.x == 0) {
-        ctl->bnorm2 = total;
-        ctl->it = 0;
-        ctl->done = 0;
-        ctl->status = 0;
-    }
-}
-
-/** If ||b|| = 0 the solution is z = 0 (the shim and this library agree on
- * that convention); zero z once the norm is known. */
-__global__ void zero_if_b_zero(double* __restrict__ z, long n, const SolveCtl* ctl) {
-    if (ctl->bnorm2 != 0.) return;
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < n; k += long(gridDim.x) * blockDim.x) z[k] = 0.;
 }
 
 __global__ void add_f32_to_f64(double* __restrict__ z, const float* __restrict__ e, long n) {
@@ -2924,15 +2906,13 @@ class MG {
 
     int enqueue_first_check(cudaStream_t s, const double* b, double* z, int precision, int use_cond,
                             cudaGraphConditionalHandle h) {
-        const long N = size(0);
-        if (precision == VDI_MG_MIXED && !general) {
-            int nb = rblocks(N);
-            norm2_kernel<<<nb, 256, 0, s>>>(b, N, rd, ctl);
-            zero_if_b_zero<<<std::min(nb, 1184), 256, 0, s>>>(z, N, ctl);
-            VDI_CUDA(cudaGetLastError());
-            return enqueue_resid32(s, b, z, 0, use_cond, h);
-        }
         int nb = sblk0();
+        if (precision == VDI_MG_MIXED && !general) {
+            if (fem()) first_check_k<double><<<nb, 256, 0, s>>>(femc<double>(0), z, b, rd, ctl, use_cond, h, b32[0]);
+            else first_check_k<double><<<nb, 256, 0, s>>>(ccc<double>(0), z, b, rd, ctl, use_cond, h, b32[0]);
+            VDI_CUDA(cudaGetLastError());
+            return VDI_OK;
+        }
         if (general)
             first_check_k<double><<<nb, 256, 0, s>>>(gen.op(0), z, b, rd, ctl, use_cond, h);
         else if (fem())

@@ -939,10 +939,8 @@ int vdi_sim_stats(vdi_sim* S, vdi_stats* out, int reset) {
     long launches = S->steps * per_step;
     for (int k = 0; k < 4; k++) {
         if (!S->mg[k]) continue;
-        // the guess kernel; the start check (mixed precision: norm, zeroing
-        // and the refinement residual)
-        const int start = S->prm.mg_precision == VDI_MG_MIXED ? 3 : 1;
-        launches += out->solves[k] * (1 + start) +
+        // the guess kernel and the start check
+        launches += out->solves[k] * 2 +
                     out->vcycles[k] * mg_kernels_per_iteration(S->mg[k], S->prm.mg_precision);
     }
     out->kernel_launches = launches;
