@@ -537,6 +537,50 @@ __global__ void k_viscous_bc(Grid g, Fields f, Gas gs) {
     }
 }
 
+/** k_viscous_bc without its barriers, over many blocks: thread t < m+4
+ * takes column t of the two bottom ghost rows, recomputing what the earlier
+ * phases would have left in the cells it reads (the mirrored ghost columns
+ * of rows 0 and 1, the u ghost rows at its neighbouring columns) by the same
+ * expressions; the threads after them mirror the left ghost columns of the
+ * rows. The values written are the single-CTA kernel's, bit for bit. */
+__global__ void k_viscous_bc_par(Grid g, Fields f, Gas gs) {
+    const int m = g.m, n = g.n, P = m + 4, ml = m + 4;
+    double* u = f.u;
+    double* v = f.v;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ml) {
+        const int j = t - ml;
+        if (!g.x_sym || j >= n) return;
+        const int c = (j + 2) * P + 2;
+        u[c - 1] = -u[c];
+        v[c - 1] = v[c];
+        u[c - 2] = -u[c + 1];
+        v[c - 2] = v[c + 1];
+        return;
+    }
+    // row r (0 or 1) of u at column k as the mirroring leaves it
+    auto urow = [&](int r, int k) -> double {
+        const int base = (2 + r) * P;
+        return (g.x_sym && k < 2) ? -u[base + 3 - k] : u[base + k];
+    };
+    // the u ghost rows -1 (lo = false) and -2 (lo = true) at column k
+    auto ughost = [&](int k, bool lo) -> double {
+        double un_edge = g.muinv * gs.tau[k];
+        return lo ? urow(1, k) - 3 * g.dy * un_edge : urow(0, k) - g.dy * un_edge;
+    };
+    const int k = t;
+    u[P + k] = ughost(k, false);
+    u[k] = ughost(k, true);
+    if (k >= 1 && k < m + 2) {
+        double uxa = 0.5 * g.xsp * (ughost(k + 1, false) - ughost(k - 1, false));
+        double uxb = 0.5 * g.xsp * (ughost(k + 1, true) - ughost(k - 1, true));
+        const double v0 = (g.x_sym && k < 2) ? v[2 * P + 3 - k] : v[2 * P + k];
+        double v1 = v0 + g.dy * uxa;
+        v[P + k] = v1;
+        v[k] = v1 + g.dy * uxb;
+    }
+}
+
 // ------------------------------------------------------- viscous sources
 // fluid_2d.cc:279-324: right-hand sides of the u and v systems.
 __global__ void k_visc_rhs(Grid g, Fields f, Gas gs, double vfx, double vfy, double* __restrict__ su,
@@ -853,7 +897,13 @@ int launch_inviscid_bc(cudaStream_t s, const Grid& g, const Fields& f, const Gas
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_viscous_bc(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs) {
-    k_viscous_bc<<<1, 1024, 0, s>>>(g, f, gs);
+    const char* e = getenv("VDI_VISC_BC_PAR");
+    if (e && atoi(e) == 0) {
+        k_viscous_bc<<<1, 1024, 0, s>>>(g, f, gs);
+    } else {
+        const int threads = (g.m + 4) + (g.x_sym ? g.n : 0);
+        k_viscous_bc_par<<<(threads + 255) / 256, 256, 0, s>>>(g, f, gs);
+    }
     return cudaGetLastError() == cudaSuccess ? VDI_OK : VDI_ERR_CUDA;
 }
 int launch_visc_rhs(cudaStream_t s, const Grid& g, const Fields& f, const Gas& gs, double vfx, double vfy,
