@@ -32,3 +32,30 @@ def test_barrier_free_viscous_bc_same_bits(sym, graph, monkeypatch):
         monkeypatch.delenv("VDI_VISC_BC_PAR")
     for k in res["0"]:
         assert np.array_equal(res["1"][k], res["0"][k]), k
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("graph", [True, False])
+def test_viscous_guesses_beside_mac_solve_same_bits(prec, graph, monkeypatch):
+    """The two viscous guesses run on the side stream beside the MAC solve,
+    extrapolating to the time the MAC correction sets (the clock the gas
+    layer left plus dt/2, the same sum the correction forms); whole runs
+    equal those with the guesses on the viscous solves' own streams
+    (VDI_VISC_GUESS_SIDE=0) bit for bit."""
+    import vdropimpact_b200 as V
+    text = open(os.path.join(HERE, "golden", "ld_vis100.cfg")).read().replace("grid_points 2048 1024",
+                                                                               "grid_points 256 128")
+    res = {}
+    for side in ("1", "0"):
+        monkeypatch.setenv("VDI_VISC_GUESS_SIDE", side)
+        f = V.Fluid2D(text, mg_rtol=1e-10, mg_precision=prec, mg_guess="quadratic", graph=graph)
+        monkeypatch.delenv("VDI_VISC_GUESS_SIDE")
+        f.init_fields()
+        f.step_forward(f.frame_dt(), 12)
+        st = f.stats()
+        res[side] = ({k: np.asarray(v).copy() for k, v in f.state().items() if k not in ("m", "n")},
+                     st["vcycles"])
+        f.close()
+    assert res["1"][1] == res["0"][1]
+    for k in res["0"][0]:
+        assert np.array_equal(res["1"][0][k], res["0"][0][k]), k

@@ -76,6 +76,9 @@ struct vdi_sim {
     float *unet_in = nullptr, *unet_out = nullptr;
     // advection stages as one fused kernel (VDI_FUSED_ADVECT=0: four kernels)
     bool fused_advect = true;
+    // the viscous guesses on the side stream beside the MAC solve
+    // (VDI_VISC_GUESS_SIDE=0: on the viscous solves' own streams)
+    bool visc_guess_side = true;
     // lift-off search (tt_analysis.cc:97-171) after every step
     LiftoffCfg lcfg{};
     LiftoffState* d_lift = nullptr;
@@ -128,9 +131,11 @@ int enqueue_step(vdi_sim* S, double dt) {
     //  - once the advection has read the ghost cells, the far-field boundary
     //    kernel (it writes only ghost velocities, which nothing before the
     //    MAC correction reads, and the gas pressure);
-    //  - the FEM guess, at the time the MAC correction will set (tadd = dt/2).
+    //  - the FEM guess, at the time the MAC correction will set (tadd = dt/2),
+    //    and the two viscous guesses, for the same time (the viscous solves
+    //    run after the correction; nothing before them reads their iterates).
     // The main stream joins before the MAC correction, which advances the
-    // clock, so the FEM guess has read it by then.
+    // clock, so the guesses have read it by then.
     // The MAC guess runs on a third stream from the start of the step: it
     // extrapolates to the time the gas layer sets (the step's starting
     // clock, copied aside first because the gas layer advances it, plus
@@ -169,6 +174,11 @@ int enqueue_step(vdi_sim* S, double dt) {
     VDI_CUDA(cudaStreamWaitEvent(S->s_gas, S->ev_adv, 0));
     VDI_TRY(launch_inviscid_bc(S->s_gas, g, S->f, S->gas, dt));
     VDI_TRY(guess(S, S->s_gas, SOLVER_FEM, S->zf, S->zf_prev, S->zf_prev2, nf, 0.5 * dt));
+    const bool vside = g.implicit_visc && S->visc_guess_side;
+    if (vside) {
+        VDI_TRY(guess(S, S->s_gas, SOLVER_VX, S->zu, S->zu_prev, S->zu_prev2, mn, 0.5 * dt));
+        VDI_TRY(guess(S, S->s_gas, SOLVER_VY, S->zv, S->zv_prev, S->zv_prev2, mn, 0.5 * dt));
+    }
     VDI_CUDA(cudaEventRecord(S->ev_side, S->s_gas));
     VDI_CUDA(cudaStreamWaitEvent(s, S->ev_guess, 0));
     if (S->prm.mg_guess == VDI_GUESS_LEARNED) {
@@ -196,9 +206,9 @@ int enqueue_step(vdi_sim* S, double dt) {
             VDI_CUDA(cudaEventRecord(S->ev_vy, s));
             VDI_CUDA(cudaStreamWaitEvent(S->s_vy, S->ev_vy, 0));
         }
-        VDI_TRY(guess(S, s, SOLVER_VX, S->zu, S->zu_prev, S->zu_prev2, mn));
+        if (!vside) VDI_TRY(guess(S, s, SOLVER_VX, S->zu, S->zu_prev, S->zu_prev2, mn));
         VDI_TRY(mg_solve_device(S->mg[SOLVER_VX], s, S->su, S->zu, prec));
-        VDI_TRY(guess(S, sv, SOLVER_VY, S->zv, S->zv_prev, S->zv_prev2, mn));
+        if (!vside) VDI_TRY(guess(S, sv, SOLVER_VY, S->zv, S->zv_prev, S->zv_prev2, mn));
         VDI_TRY(mg_solve_device(S->mg[SOLVER_VY], sv, S->sv, S->zv, prec));
         if (par) {
             VDI_CUDA(cudaEventRecord(S->ev_vy_done, S->s_vy));
@@ -485,6 +495,7 @@ int vdi_sim_create(const vdi_params* prm, void* stream, vdi_sim** out) {
     g.m = P.m; g.n = P.n; g.x_sym = P.x_sym; g.implicit_visc = P.implicit_visc;
     g.blk_x = 32; g.blk_y = 8;
     if (const char* e = getenv("VDI_FUSED_ADVECT")) S->fused_advect = atoi(e) != 0;
+    if (const char* e = getenv("VDI_VISC_GUESS_SIDE")) S->visc_guess_side = atoi(e) != 0;
     g.ax = P.ax; g.ay = P.ay; g.bx = P.bx; g.by = P.by;
     // fluid_2d.cc:15-17
     g.dx = (P.bx - P.ax) / P.m;
