@@ -229,8 +229,12 @@ __global__ void k_stage5_src(Grid g, Fields f, Gas gs, double dt, double* __rest
 // computed by the same expressions as in the four kernels, so the results
 // are bit-identical.
 namespace {
-constexpr int ADV_TX = 32, ADV_TY = 16, ADV_NT = ADV_TX * ADV_TY;
+constexpr int ADV_TX = 32, ADV_TY = 16;
 constexpr int ADV_W = ADV_TX + 4, ADV_H = ADV_TY + 4, ADV_N = ADV_W * ADV_H;   // edge windows
+// threads of a CTA: at least one per edge-window cell, so each stage is one
+// pass (23 warps; stage 5 uses the first TX x TY of them)
+constexpr int ADV_NT = (ADV_N + 31) / 32 * 32;
+static_assert(ADV_NT >= ADV_TX * ADV_TY, "stage 5 takes one tile cell per thread");
 constexpr int ADV_UW = ADV_TX + 8, ADV_UH = ADV_TY + 8;                        // u, v window
 constexpr int ADV_PW = ADV_TX + 3, ADV_PH = ADV_TY + 3;                        // pressure nodes
 constexpr size_t ADV_SMEM = (size_t(16) * ADV_N + 2 * ADV_UW * ADV_UH + ADV_PW * ADV_PH) * sizeof(double);
@@ -350,6 +354,7 @@ __global__ void __launch_bounds__(ADV_NT) k_advect(Grid g, Fields f, double dt, 
     __syncthreads();
     // ---- stage 5 (k_stage5_src without the bottom gas term) on the tile
     {
+        if (tid >= ADV_TX * ADV_TY) return;
         const int a = 2 + tid % ADV_TX, b = 2 + tid / ADV_TX, i = ox + a, j = oy + b;
         if (i >= m || j >= n) return;
         const int t = b * ADV_W + a;
